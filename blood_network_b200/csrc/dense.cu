@@ -1,0 +1,106 @@
+// Coarsest-level solve: dense FP64 Cholesky, then the explicit inverse, so
+// that each V-cycle's coarse solve is one dense matrix-vector product.
+//
+// The reference solves the coarsest level with ichol-preconditioned PCG to a
+// relative B-norm of 1e-12 (C_amg1/src/amg_cycle.c:188,229); a direct solve
+// reaches the exact coarse solution up to cond(A_c) * eps.  The coarse
+// operator is SPD (Galerkin product of an SPD matrix), so Cholesky applies.
+#include "dense.cuh"
+
+namespace bn {
+
+__global__ void k_csr_to_dense(const int* __restrict__ ia, const int* __restrict__ ja,
+                               const double* __restrict__ val, int n, double* __restrict__ D) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = ia[i]; k < ia[i + 1]; k++) D[(size_t)i * n + ja[k]] += val[k];
+}
+
+// column j: pivot and scale (one block)
+__global__ void k_chol_col(double* D, int n, int j, int* err) {
+  __shared__ double piv;
+  if (threadIdx.x == 0) {
+    double d = D[(size_t)j * n + j];
+    if (!(d > 0.0)) {
+      atomicCAS(err, 0, 1);
+      d = 1e-300;
+    }
+    piv = sqrt(d);
+    D[(size_t)j * n + j] = piv;
+  }
+  __syncthreads();
+  const double inv = 1.0 / piv;
+  for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) D[(size_t)i * n + j] *= inv;
+}
+
+// trailing update of the lower triangle: D[i][k] -= L[i][j] L[k][j], j<k<=i
+__global__ void k_chol_update(double* D, int n, int j) {
+  const int m = n - j - 1;
+  const long long total = (long long)m * m;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    int i = j + 1 + (int)(t / m);
+    int k = j + 1 + (int)(t % m);
+    if (k <= i) D[(size_t)i * n + k] -= D[(size_t)i * n + j] * D[(size_t)k * n + j];
+  }
+}
+
+// column c of A^{-1} = L^{-T} L^{-1} e_c, one thread per column, in place
+__global__ void k_chol_inverse(const double* __restrict__ L, int n, double* __restrict__ X) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    for (int i = 0; i < c; i++) X[(size_t)i * n + c] = 0.0;
+    for (int i = c; i < n; i++) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; k++) s -= L[(size_t)i * n + k] * X[(size_t)k * n + c];
+      X[(size_t)i * n + c] = s / L[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+      double s = X[(size_t)i * n + c];
+      for (int k = i + 1; k < n; k++) s -= L[(size_t)k * n + i] * X[(size_t)k * n + c];
+      X[(size_t)i * n + c] = s / L[(size_t)i * n + i];
+    }
+  }
+}
+
+// x = Ainv b; one warp per row, FP64 accumulation
+template <class T>
+__global__ void k_dense_apply(const double* __restrict__ Ainv, int n, const T* __restrict__ b,
+                              T* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const double* row = Ainv + (size_t)i * n;
+    double s = 0.0;
+    for (int k = lane; k < n; k += 32) s += row[k] * (double)b[k];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) x[i] = (T)s;
+  }
+}
+
+void DenseCoarse::setup(const CSR& A, cudaStream_t s) {
+  n = A.n;
+  BN_REQUIRE(n <= kDenseMax, BN_ERR_COARSE, "coarsest level too large for the dense solve");
+  DBuf<double> D((size_t)n * n, s);
+  D.zero();
+  DBuf<int> err(1, s);
+  err.zero();
+  if (n > 0) BN_LAUNCH(k_csr_to_dense, grid_for(n, 128), 128, 0, s, A.ia.p, A.ja.p, A.val.p, n, D.p);
+  for (int j = 0; j < n; j++) {
+    BN_LAUNCH(k_chol_col, 1, 256, 0, s, D.p, n, j, err.p);
+    long long m = (long long)(n - j - 1) * (n - j - 1);
+    if (m > 0) BN_LAUNCH(k_chol_update, grid_for(m, 256), 256, 0, s, D.p, n, j);
+  }
+  BN_REQUIRE(read_scalar(err.p, s) == 0, BN_ERR_COARSE,
+             "coarsest operator is not positive definite");
+  inv.alloc((size_t)n * n, s);
+  if (n > 0) BN_LAUNCH(k_chol_inverse, grid_for(n, 64, 4), 64, 0, s, D.p, n, inv.p);
+}
+
+template <class T>
+void DenseCoarse::apply(const T* b, T* x, cudaStream_t s) const {
+  if (n == 0) return;
+  BN_LAUNCH(k_dense_apply<T>, grid_for((long long)n * 32, 256, 8), 256, 0, s, inv.p, n, b, x);
+}
+template void DenseCoarse::apply<double>(const double*, double*, cudaStream_t) const;
+template void DenseCoarse::apply<float>(const float*, float*, cudaStream_t) const;
+
+}  // namespace bn

@@ -1,0 +1,523 @@
+// IC(0) on the device: factorization and the two triangular solves.
+//
+// Follows ichol_compute / ichol_solve (C_amg1/src/ichol.c:12-165):
+//  * L takes A's lower triangle (j <= i) in A's in-row order.
+//  * Row i, in storage order, for each k < i:
+//      L(i,k) = (w_k - sum_{j in pre(k), j in row i} w_j L(k,j)) / L(k,k)
+//    where pre(k) is the leading part of row k before its first column
+//    >= k (the reference breaks there) and w holds row i's current values.
+//    Then L(i,i) = sqrt(w_i - sum_{j in pre(i)} w_j^2), a non-positive
+//    pivot becomes 1e-14 (:102).
+//  * Forward: y_i = (b_i - sum_{j<i} L(i,j) y_j) / L(i,i), row order.
+//  * Backward (column oriented in the reference): x_j = (y_j - sum over
+//    i > j, in decreasing i, of L(i,j) x_i) / L(j,j).
+// Every row is computed by one thread in that exact operation order, so the
+// factor and the solves are bit-identical to the reference.
+//
+// Parallel schedule: row i depends on the rows k < i of its own pattern.
+// Dependency levels come from a Kahn frontier sweep (level l = rows whose
+// dependencies all lie in levels < l); rows are stored and processed in
+// level order.  Each level is one launch; runs of consecutive narrow levels
+// (tree parts, lattice corners) are batched into a single 1024-thread block
+// that steps through them with __syncthreads().  There are no cross-block
+// waits anywhere, so nothing can spin.
+#include "ichol.cuh"
+
+#include <cub/cub.cuh>
+
+namespace bn {
+
+constexpr int kNarrow = 2048;     // levels up to this width are batched
+constexpr int kBatchThreads = 1024;
+
+// ---------------------------------------------------------------- pattern
+__global__ void k_lower_count(const int* __restrict__ ia, const int* __restrict__ ja, int n,
+                              int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int c = 0;
+    for (int k = ia[i]; k < ia[i + 1]; k++) c += (ja[k] <= i);
+    cnt[i] = c;
+  }
+}
+
+// extract the lower triangle; pre = leading entries with col < i; dpos =
+// first diagonal position (-1 if missing)
+__global__ void k_lower_fill(const int* __restrict__ ia, const int* __restrict__ ja,
+                             const double* __restrict__ val, int n, const int* __restrict__ lia,
+                             int* __restrict__ lja, double* __restrict__ lval,
+                             int* __restrict__ pre, int* __restrict__ dpos, int* flags) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int p = lia[i];
+    for (int k = ia[i]; k < ia[i + 1]; k++) {
+      int j = ja[k];
+      if (j <= i) {
+        lja[p] = j;
+        lval[p] = val[k];
+        p++;
+      }
+    }
+    int q = 0;
+    while (lia[i] + q < lia[i + 1] && lja[lia[i] + q] < i) q++;
+    pre[i] = q;
+    int d = -1;
+    for (int k = lia[i]; k < lia[i + 1]; k++)
+      if (lja[k] == i) { d = k; break; }
+    dpos[i] = d;
+    if (d < 0) atomicOr(flags, 1);
+  }
+}
+
+// pre/dpos for a factor given directly (every entry must satisfy j <= i)
+__global__ void k_factor_meta(const int* __restrict__ lia, const int* __restrict__ lja, int n,
+                              int* __restrict__ pre, int* __restrict__ dpos, int* flags) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int q = 0;
+    while (lia[i] + q < lia[i + 1] && lja[lia[i] + q] < i) q++;
+    pre[i] = q;
+    int d = -1;
+    for (int k = lia[i]; k < lia[i + 1]; k++) {
+      if (lja[k] > i) atomicOr(flags, 2);
+      if (lja[k] == i && d < 0) d = k;
+    }
+    dpos[i] = d;
+    if (d < 0) atomicOr(flags, 1);
+  }
+}
+
+// strict lower part as CSR; values carry source positions in L (exact in double)
+__global__ void k_strict_count(const int* __restrict__ lia, const int* __restrict__ lja, int n,
+                               int* __restrict__ cnt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int c = 0;
+    for (int k = lia[i]; k < lia[i + 1]; k++) c += (lja[k] < i);
+    cnt[i] = c;
+  }
+}
+__global__ void k_strict_fill(const int* __restrict__ lia, const int* __restrict__ lja, int n,
+                              const int* __restrict__ sia, int* __restrict__ sja,
+                              double* __restrict__ ssrc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int p = sia[i];
+    for (int k = lia[i]; k < lia[i + 1]; k++)
+      if (lja[k] < i) { sja[p] = lja[k]; ssrc[p] = (double)k; p++; }
+  }
+}
+
+// ---------------------------------------------------------------- levels
+__global__ void k_indeg(const int* __restrict__ sia, int n, int* __restrict__ indeg,
+                        int* __restrict__ level, int* __restrict__ frontier, int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int d = sia[i + 1] - sia[i];
+    indeg[i] = d;
+    if (d == 0) {
+      level[i] = 0;
+      frontier[atomicAdd(counter, 1)] = i;
+    }
+  }
+}
+
+// one Kahn step: rows of the current frontier release their dependents
+__global__ void k_kahn_step(const int* __restrict__ uia, const int* __restrict__ uja,
+                            const int* __restrict__ cur, int m, int lev, int* __restrict__ indeg,
+                            int* __restrict__ level, int* __restrict__ next, int* counter) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+    const int k = cur[t];
+    for (int q = uia[k]; q < uia[k + 1]; q++) {
+      const int i = uja[q];
+      if (atomicSub(&indeg[i], 1) == 1) {
+        level[i] = lev;
+        next[atomicAdd(counter, 1)] = i;
+      }
+    }
+  }
+}
+
+__global__ void k_iota_i(int* a, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+// ---------------------------------------------------------------- factor
+__device__ __forceinline__ void ic_factor_row(int i, const int* __restrict__ lia,
+                                              const int* __restrict__ lja, double* lval,
+                                              const int* __restrict__ pre,
+                                              const int* __restrict__ dpos) {
+  const int r0 = lia[i], r1 = lia[i + 1];
+  for (int kk = r0; kk < r1; kk++) {
+    const int k = lja[kk];
+    if (k >= i) continue;
+    double s = lval[kk];
+    const int k0 = lia[k], kp = k0 + pre[k];
+    for (int jj = k0; jj < kp; jj++) {
+      const int j = lja[jj];
+      for (int q = r0; q < r1; q++) {  // is j in row i?  (w_marker)
+        if (lja[q] == j) {
+          s = xsub(s, xmul(lval[q], lval[jj]));
+          break;
+        }
+      }
+    }
+    lval[kk] = xdiv(s, lval[dpos[k]]);
+  }
+  const int di = dpos[i];
+  double d = lval[di];
+  for (int q = r0; q < r0 + pre[i]; q++) d = xsub(d, xmul(lval[q], lval[q]));
+  if (d <= 0.0) d = 1e-14;
+  lval[di] = __dsqrt_rn(d);
+}
+
+__global__ void k_ic_factor_wide(const int* __restrict__ lia, const int* __restrict__ lja,
+                                 double* lval, const int* __restrict__ pre,
+                                 const int* __restrict__ dpos, const int* __restrict__ order,
+                                 int t0, int t1) {
+  for (int t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t < t1; t += gridDim.x * blockDim.x)
+    ic_factor_row(order[t], lia, lja, lval, pre, dpos);
+}
+
+__global__ void __launch_bounds__(kBatchThreads)
+k_ic_factor_batch(const int* __restrict__ lia, const int* __restrict__ lja, double* lval,
+                  const int* __restrict__ pre, const int* __restrict__ dpos,
+                  const int* __restrict__ order, const int* __restrict__ lptr, int l0, int l1) {
+  for (int l = l0; l < l1; l++) {
+    for (int t = lptr[l] + threadIdx.x; t < lptr[l + 1]; t += blockDim.x)
+      ic_factor_row(order[t], lia, lja, lval, pre, dpos);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- solves
+// Row t of a layout: output index rows[t], entries [ia[t], ia[t+1]) of
+// (column, value), divisor diag[t]:  out = (in - sum val*x[col]) / diag.
+// x is read and written in the same kernel, so it is never marked
+// read-only.
+template <class T>
+__device__ __forceinline__ void tri_row(int t, const int* __restrict__ ia,
+                                        const int* __restrict__ ja, const T* __restrict__ val,
+                                        const T* __restrict__ diag, const int* __restrict__ rows,
+                                        const T* __restrict__ in, T* x) {
+  const int i = rows[t];
+  T s = in[i];
+  for (int k = ia[t]; k < ia[t + 1]; k++) {
+    if constexpr (sizeof(T) == 8)
+      s = xsub(s, xmul(val[k], x[ja[k]]));
+    else
+      s = xsubf(s, xmulf(val[k], x[ja[k]]));
+  }
+  x[i] = s / diag[t];
+}
+
+template <class T>
+__global__ void k_tri_wide(const int* __restrict__ ia, const int* __restrict__ ja,
+                           const T* __restrict__ val, const T* __restrict__ diag,
+                           const int* __restrict__ rows, int t0, int t1, const T* __restrict__ in,
+                           T* x) {
+  for (int t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t < t1; t += gridDim.x * blockDim.x)
+    tri_row<T>(t, ia, ja, val, diag, rows, in, x);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBatchThreads)
+k_tri_batch(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+            const T* __restrict__ diag, const int* __restrict__ rows,
+            const int* __restrict__ lptr, int l0, int l1, const T* __restrict__ in, T* x) {
+  for (int l = l0; l < l1; l++) {
+    for (int t = lptr[l] + threadIdx.x; t < lptr[l + 1]; t += blockDim.x)
+      tri_row<T>(t, ia, ja, val, diag, rows, in, x);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- layout
+__global__ void k_fwd_count(const int* __restrict__ lia, const int* __restrict__ lja,
+                            const int* __restrict__ order, int n, int* __restrict__ cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int i = order[t], c = 0;
+    for (int k = lia[i]; k < lia[i + 1]; k++) c += (lja[k] < i);
+    cnt[t] = c;
+  }
+}
+
+__global__ void k_fwd_fill(const int* __restrict__ lia, const int* __restrict__ lja,
+                           const int* __restrict__ order, int n, const int* __restrict__ fia,
+                           int* __restrict__ fja, int* __restrict__ fsrc) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int i = order[t], p = fia[t];
+    for (int k = lia[i]; k < lia[i + 1]; k++)
+      if (lja[k] < i) { fja[p] = lja[k]; fsrc[p] = k; p++; }
+  }
+}
+
+__global__ void k_bwd_count(const int* __restrict__ uia, const int* __restrict__ border, int n,
+                            int* __restrict__ cnt) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int j = border[t];
+    cnt[t] = uia[j + 1] - uia[j];
+  }
+}
+
+// U row j lists i > j ascending (stable transpose); stored descending
+__global__ void k_bwd_fill(const int* __restrict__ uia, const int* __restrict__ uja,
+                           const int* __restrict__ usrc, const int* __restrict__ border, int n,
+                           const int* __restrict__ bia, int* __restrict__ bja,
+                           int* __restrict__ bsrc) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int j = border[t], p = bia[t];
+    for (int k = uia[j + 1] - 1; k >= uia[j]; k--) { bja[p] = uja[k]; bsrc[p] = usrc[k]; p++; }
+  }
+}
+
+__global__ void k_reverse(const int* __restrict__ a, int n, int* __restrict__ b) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    b[t] = a[n - 1 - t];
+}
+
+template <class T>
+__global__ void k_gather_vals(const int* __restrict__ src, int m, const double* __restrict__ lval,
+                              T* __restrict__ out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
+    out[p] = (T)lval[src[p]];
+}
+
+template <class T>
+__global__ void k_gather_diag(const int* __restrict__ order, int n, const int* __restrict__ dpos,
+                              const double* __restrict__ lval, T* __restrict__ out) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    out[t] = (T)lval[dpos[order[t]]];
+}
+
+__global__ void k_double_to_int(const double* __restrict__ a, int m, int* __restrict__ b) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
+    b[p] = (int)a[p];
+}
+
+// ---------------------------------------------------------------- host
+// Segments: a wide level is one grid launch; a run of narrow levels is one
+// batched block.  Built from host level offsets.
+static void make_segments(const std::vector<int>& ptr, std::vector<IChol::Seg>& segs) {
+  segs.clear();
+  const int nl = (int)ptr.size() - 1;
+  int l = 0;
+  while (l < nl) {
+    int w = ptr[l + 1] - ptr[l];
+    if (w > kNarrow) {
+      segs.push_back({0, l, l + 1, ptr[l], ptr[l + 1]});
+      l++;
+    } else {
+      int l1 = l;
+      while (l1 < nl && ptr[l1 + 1] - ptr[l1] <= kNarrow) l1++;
+      segs.push_back({1, l, l1, ptr[l], ptr[l1]});
+      l = l1;
+    }
+  }
+}
+
+void IChol::factor(const CSR& A, cudaStream_t s) {
+  stream = s;
+  n = A.n;
+  const int g = grid_for(n, 256);
+  DBuf<int> cnt((size_t)n + 1, s);
+  cnt.zero();
+  BN_LAUNCH(k_lower_count, g, 256, 0, s, A.ia.p, A.ja.p, n, cnt.p);
+  int lnnz = scan_counts(cnt.p, n, s);
+  L.n = L.m = n;
+  L.nnz = lnnz;
+  L.ia = std::move(cnt);
+  L.ja.alloc((size_t)(lnnz > 0 ? lnnz : 1), s);
+  L.val.alloc((size_t)(lnnz > 0 ? lnnz : 1), s);
+  finish(A.ia.p, A.ja.p, A.val.p, true, s);
+}
+
+void IChol::load(CSR&& Lf, cudaStream_t s) {
+  stream = s;
+  n = Lf.n;
+  L = std::move(Lf);
+  finish(L.ia.p, L.ja.p, L.val.p, false, s);
+}
+
+// Lower-triangle extraction (from A, or checks on a given factor), the
+// dependency levels, the numeric factorization and the solve layouts.
+void IChol::finish(const int* aia, const int* aja, const double* aval, bool numeric,
+                   cudaStream_t s) {
+  const int g = grid_for(n, 256);
+  DBuf<int> flags(1, s);
+  flags.zero();
+  pre.alloc(n, s);
+  dpos.alloc(n, s);
+  if (numeric) {
+    BN_LAUNCH(k_lower_fill, g, 256, 0, s, aia, aja, aval, n, L.ia.p, L.ja.p, L.val.p, pre.p,
+              dpos.p, flags.p);
+  } else {
+    BN_LAUNCH(k_factor_meta, g, 256, 0, s, L.ia.p, L.ja.p, n, pre.p, dpos.p, flags.p);
+  }
+  int f = read_scalar(flags.p, s);
+  BN_REQUIRE(!(f & 1), BN_ERR_ARG, "IC(0): a row has no diagonal entry");
+  BN_REQUIRE(!(f & 2), BN_ERR_ARG, "IC(0): factor holds an entry above the diagonal");
+
+  // strict lower part and its transpose (the dependents of each row)
+  CSR Sl, U;
+  {
+    DBuf<int> c((size_t)n + 1, s);
+    c.zero();
+    BN_LAUNCH(k_strict_count, g, 256, 0, s, L.ia.p, L.ja.p, n, c.p);
+    int snnz = scan_counts(c.p, n, s);
+    Sl.n = Sl.m = n;
+    Sl.nnz = snnz;
+    Sl.ia = std::move(c);
+    Sl.ja.alloc((size_t)(snnz > 0 ? snnz : 1), s);
+    Sl.val.alloc((size_t)(snnz > 0 ? snnz : 1), s);
+    BN_LAUNCH(k_strict_fill, g, 256, 0, s, L.ia.p, L.ja.p, n, Sl.ia.p, Sl.ja.p, Sl.val.p);
+    transpose(Sl, U, s, true);
+  }
+  offd_nnz = Sl.nnz;
+
+  // Kahn frontier sweep -> level of every row
+  {
+    Phase ph("ichol levels", s);
+    DBuf<int> indeg(n, s), level(n, s), frontier(n, s), ctr(1, s);
+    ctr.zero();
+    BN_LAUNCH(k_indeg, g, 256, 0, s, Sl.ia.p, n, indeg.p, level.p, frontier.p, ctr.p);
+    int lo = 0, hi = read_scalar(ctr.p, s);
+    int lev = 0;
+    while (hi > lo) {
+      lev++;
+      BN_LAUNCH(k_kahn_step, grid_for(hi - lo, 256), 256, 0, s, U.ia.p, U.ja.p, frontier.p + lo,
+                hi - lo, lev, indeg.p, level.p, frontier.p, ctr.p);
+      lo = hi;
+      hi = read_scalar(ctr.p, s);
+    }
+    BN_REQUIRE(hi == n, BN_ERR_ARG, "IC(0): dependency levels did not cover every row");
+    nlevels = lev;
+    // level order, stable (natural order within a level)
+    order.alloc(n, s);
+    DBuf<int> ids(n, s), keys_out(n, s);
+    BN_LAUNCH(k_iota_i, g, 256, 0, s, ids.p, n);
+    size_t tmp = 0;
+    int eb = 1;
+    while ((1LL << eb) <= (long long)nlevels) eb++;
+    BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, level.p, keys_out.p, ids.p, order.p, n,
+                                            0, eb, s));
+    DBuf<unsigned char> t(tmp, s);
+    BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, level.p, keys_out.p, ids.p, order.p, n, 0,
+                                            eb, s));
+    // level offsets
+    std::vector<int> hk(n);
+    keys_out.download(hk.data(), n);
+    BN_CUDA(cudaStreamSynchronize(s));
+    lptr.assign(nlevels + 1, 0);
+    for (int i = 0; i < n; i++) lptr[hk[i] + 1]++;
+    for (int l = 0; l < nlevels; l++) lptr[l + 1] += lptr[l];
+  }
+  // backward processing order: reverse level order
+  border.alloc(n, s);
+  BN_LAUNCH(k_reverse, g, 256, 0, s, order.p, n, border.p);
+  bptr.assign(nlevels + 1, 0);
+  for (int l = 0; l <= nlevels; l++) bptr[l] = n - lptr[nlevels - l];
+  make_segments(lptr, fseg);
+  make_segments(bptr, bseg);
+  d_lptr.alloc(nlevels + 1, s);
+  d_lptr.upload(lptr.data(), nlevels + 1);
+  d_bptr.alloc(nlevels + 1, s);
+  d_bptr.upload(bptr.data(), nlevels + 1);
+
+  if (numeric) {
+    Phase ph("ichol numeric", s);
+    for (const Seg& sg : fseg) {
+      if (sg.kind == 0)
+        BN_LAUNCH(k_ic_factor_wide, grid_for(sg.t1 - sg.t0, 128), 128, 0, s, L.ia.p, L.ja.p,
+                  L.val.p, pre.p, dpos.p, order.p, sg.t0, sg.t1);
+      else
+        BN_LAUNCH(k_ic_factor_batch, 1, kBatchThreads, 0, s, L.ia.p, L.ja.p, L.val.p, pre.p,
+                  dpos.p, order.p, d_lptr.p, sg.l0, sg.l1);
+    }
+  }
+
+  // forward solve layout (level order)
+  fia.alloc((size_t)n + 1, s);
+  fia.zero();
+  BN_LAUNCH(k_fwd_count, g, 256, 0, s, L.ia.p, L.ja.p, order.p, n, fia.p);
+  int fnnz = scan_counts(fia.p, n, s);
+  fja.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
+  fsrc.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
+  BN_LAUNCH(k_fwd_fill, g, 256, 0, s, L.ia.p, L.ja.p, order.p, n, fia.p, fja.p, fsrc.p);
+  // backward solve layout (reverse level order), rows of U = (strict L)^T
+  {
+    DBuf<int> usrc((size_t)(fnnz > 0 ? fnnz : 1), s);
+    if (fnnz > 0)
+      BN_LAUNCH(k_double_to_int, grid_for(fnnz, 256), 256, 0, s, U.val.p, fnnz, usrc.p);
+    bia.alloc((size_t)n + 1, s);
+    bia.zero();
+    BN_LAUNCH(k_bwd_count, g, 256, 0, s, U.ia.p, border.p, n, bia.p);
+    scan_counts(bia.p, n, s);
+    bja.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
+    bsrc.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
+    BN_LAUNCH(k_bwd_fill, g, 256, 0, s, U.ia.p, U.ja.p, usrc.p, border.p, n, bia.p, bja.p, bsrc.p);
+  }
+  refresh_values();
+}
+
+void IChol::refresh_values() {
+  cudaStream_t s = stream;
+  const int g = grid_for(n, 256);
+  const int m = offd_nnz > 0 ? offd_nnz : 1;
+  fval.alloc(m, s);
+  bval.alloc(m, s);
+  fdiag.alloc(n, s);
+  bdiag.alloc(n, s);
+  if (offd_nnz > 0) {
+    BN_LAUNCH(k_gather_vals<double>, grid_for(offd_nnz, 256), 256, 0, s, fsrc.p, offd_nnz,
+              L.val.p, fval.p);
+    BN_LAUNCH(k_gather_vals<double>, grid_for(offd_nnz, 256), 256, 0, s, bsrc.p, offd_nnz,
+              L.val.p, bval.p);
+  }
+  BN_LAUNCH(k_gather_diag<double>, g, 256, 0, s, order.p, n, dpos.p, L.val.p, fdiag.p);
+  BN_LAUNCH(k_gather_diag<double>, g, 256, 0, s, border.p, n, dpos.p, L.val.p, bdiag.p);
+  if (want_f32) {
+    fval32.alloc(m, s);
+    bval32.alloc(m, s);
+    fdiag32.alloc(n, s);
+    bdiag32.alloc(n, s);
+    if (offd_nnz > 0) {
+      BN_LAUNCH(k_gather_vals<float>, grid_for(offd_nnz, 256), 256, 0, s, fsrc.p, offd_nnz,
+                L.val.p, fval32.p);
+      BN_LAUNCH(k_gather_vals<float>, grid_for(offd_nnz, 256), 256, 0, s, bsrc.p, offd_nnz,
+                L.val.p, bval32.p);
+    }
+    BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, order.p, n, dpos.p, L.val.p, fdiag32.p);
+    BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, border.p, n, dpos.p, L.val.p, bdiag32.p);
+  }
+}
+
+template <class T>
+static void run_tri(const std::vector<IChol::Seg>& segs, const int* ia, const int* ja,
+                    const T* val, const T* diag, const int* rows, const int* dptr, const T* in,
+                    T* x, cudaStream_t s) {
+  for (const IChol::Seg& sg : segs) {
+    if (sg.kind == 0)
+      BN_LAUNCH(k_tri_wide<T>, grid_for(sg.t1 - sg.t0, 128), 128, 0, s, ia, ja, val, diag, rows,
+                sg.t0, sg.t1, in, x);
+    else
+      BN_LAUNCH(k_tri_batch<T>, 1, kBatchThreads, 0, s, ia, ja, val, diag, rows, dptr, sg.l0,
+                sg.l1, in, x);
+  }
+}
+
+template <class T>
+void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
+  const T* fv;
+  const T* fd;
+  const T* bv;
+  const T* bd;
+  if constexpr (sizeof(T) == 8) {
+    fv = fval.p; fd = fdiag.p; bv = bval.p; bd = bdiag.p;
+  } else {
+    fv = fval32.p; fd = fdiag32.p; bv = bval32.p; bd = bdiag32.p;
+  }
+  run_tri<T>(fseg, fia.p, fja.p, fv, fd, order.p, d_lptr.p, b, y, s);
+  run_tri<T>(bseg, bia.p, bja.p, bv, bd, border.p, d_bptr.p, y, x, s);
+}
+
+template void IChol::solve<double>(const double*, double*, double*, cudaStream_t);
+template void IChol::solve<float>(const float*, float*, float*, cudaStream_t);
+
+int IChol::take_error(cudaStream_t) { return 0; }
+
+}  // namespace bn

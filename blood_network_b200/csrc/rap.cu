@@ -1,0 +1,657 @@
+// Galerkin coarse operator Ac = R A P (R = P^T) as a two-pass SpGEMM with
+// hash accumulators: pass 1 counts the distinct columns of every coarse row,
+// a scan sizes Ac, pass 2 fills it.
+//
+// Bit-exact with dcsr_rap (C_amg1/src/sparse_ops.c:102-213).  The reference
+// walks R row ic, then A row i1, then P row i2 in storage order, forms
+// (r * a) * p and accumulates in that order; row ic starts with its diagonal
+// (value 0.0, then accumulated), the other columns follow in order of first
+// discovery and start from their first product.
+//
+// Layout: one warp per coarse row.  Pass 1 inserts the product columns of
+// the row into a shared-memory open-addressing table in parallel
+// (atomicCAS) and counts the new keys.  Pass 2 keeps the reference's
+// sequential order without serialising the memory traffic: the 32 lanes walk
+// A row i1 together (coalesced), form r*a, expand their P rows into an
+// ordered product stream in shared memory (warp prefix sum), and lane 0
+// consumes the stream in order -- column -> slot lookup, first product
+// assigned, later ones added -- so every sum is formed in exactly the
+// reference's order.  Rows whose column count exceeds the per-warp table use
+// a one-warp block with a large dynamic table, and beyond that a table in
+// global memory.
+#include "internal.cuh"
+
+#include <cub/cub.cuh>
+
+namespace bn {
+
+constexpr int kWarpCap = 1024;    // per-warp table (distinct columns <= 512)
+constexpr int kBigCap = 8192;     // one-warp-per-block table (<= 4096)
+constexpr int kRapWarps = 4;
+constexpr int kBuf = 256;         // product stream chunk
+
+__device__ __forceinline__ unsigned rap_hash(int key, unsigned mask) {
+  return ((unsigned)key * 2654435761u >> 7) & mask;
+}
+
+struct Table {
+  int* keys;
+  int* slots;     // fill pass only
+  double* vals;   // fill pass only (indexed by slot)
+  unsigned mask;
+};
+
+__device__ __forceinline__ void table_clear(Table t, int lane) {
+  for (unsigned e = lane; e <= t.mask; e += 32) t.keys[e] = -1;
+}
+
+// parallel insert; true if this call inserted the key
+__device__ __forceinline__ bool table_insert_atomic(Table t, int key) {
+  unsigned h = rap_hash(key, t.mask);
+  while (true) {
+    int prev = atomicCAS(&t.keys[h], -1, key);
+    if (prev == -1) return true;
+    if (prev == key) return false;
+    h = (h + 1) & t.mask;
+  }
+}
+
+// sequential (single lane) find-or-insert; returns the slot
+__device__ __forceinline__ int table_slot(Table t, int key, int new_slot, bool* inserted) {
+  unsigned h = rap_hash(key, t.mask);
+  while (true) {
+    int k = t.keys[h];
+    if (k == key) { *inserted = false; return t.slots[h]; }
+    if (k == -1) {
+      t.keys[h] = key;
+      t.slots[h] = new_slot;
+      *inserted = true;
+      return new_slot;
+    }
+    h = (h + 1) & t.mask;
+  }
+}
+
+// product-count bound per coarse row: 1 (diagonal) + sum |P_i2|
+__global__ void k_rap_bound(const int* __restrict__ ria, const int* __restrict__ rja,
+                            const int* __restrict__ aia, const int* __restrict__ aja,
+                            const int* __restrict__ pia, int nc, long long* __restrict__ ub) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ic < nc; ic += warps) {
+    long long b = 0;
+    for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
+      int i1 = rja[k1];
+      for (int k2 = aia[i1] + lane; k2 < aia[i1 + 1]; k2 += 32) {
+        int i2 = aja[k2];
+        b += pia[i2 + 1] - pia[i2];
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) b += __shfl_xor_sync(0xffffffffu, b, off);
+    if (lane == 0) ub[ic] = 1 + b;
+  }
+}
+
+__device__ int rap_count_row(int ic, Table t, int lane, const int* __restrict__ ria,
+                             const int* __restrict__ rja, const int* __restrict__ aia,
+                             const int* __restrict__ aja, const int* __restrict__ pia,
+                             const int* __restrict__ pja) {
+  table_clear(t, lane);
+  __syncwarp();
+  int cnt = 0;
+  if (lane == 0) cnt += table_insert_atomic(t, ic);
+  for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
+    const int i1 = rja[k1];
+    for (int k2 = aia[i1] + lane; k2 < aia[i1 + 1]; k2 += 32) {
+      const int i2 = aja[k2];
+      for (int k3 = pia[i2]; k3 < pia[i2 + 1]; k3++) cnt += table_insert_atomic(t, pja[k3]);
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+  __syncwarp();
+  return cnt;
+}
+
+__device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
+                             const int* __restrict__ ria, const int* __restrict__ rja,
+                             const double* __restrict__ rval, const int* __restrict__ aia,
+                             const int* __restrict__ aja, const double* __restrict__ aval,
+                             const int* __restrict__ pia, const int* __restrict__ pja,
+                             const double* __restrict__ pval, int cbase, int* __restrict__ cja,
+                             double* __restrict__ cval) {
+  table_clear(t, lane);
+  __syncwarp();
+  int nslots = 0;
+  if (lane == 0) {
+    bool ins;
+    table_slot(t, ic, 0, &ins);
+    t.vals[0] = 0.0;
+    cja[cbase] = ic;
+    nslots = 1;
+  }
+  const unsigned lt = (1u << lane) - 1u;
+  for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
+    const double r = rval[k1];
+    const int i1 = rja[k1];
+    const int a1 = aia[i1 + 1];
+    for (int base = aia[i1]; base < a1; base += 32) {
+      const int k2 = base + lane;
+      double ra = 0.0;
+      int p0 = 0, plen = 0;
+      if (k2 < a1) {
+        ra = xmul(r, aval[k2]);
+        const int i2 = aja[k2];
+        p0 = pia[i2];
+        plen = pia[i2 + 1] - p0;
+      }
+      // exclusive prefix of plen across the warp (stream positions)
+      int incl = plen;
+      for (int off = 1; off < 32; off <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int start = incl - plen;
+      (void)lt;
+      for (int cs = 0; cs < total; cs += kBuf) {
+        for (int q = 0; q < plen; q++) {
+          const int sidx = start + q - cs;
+          if (sidx >= 0 && sidx < kBuf) {
+            bcol[sidx] = pja[p0 + q];
+            bval[sidx] = xmul(ra, pval[p0 + q]);
+          }
+        }
+        __syncwarp();
+        if (lane == 0) {
+          const int m = min(kBuf, total - cs);
+          for (int q = 0; q < m; q++) {
+            const int col = bcol[q];
+            const double v = bval[q];
+            bool ins;
+            const int slot = table_slot(t, col, nslots, &ins);
+            if (ins) {
+              t.vals[slot] = v;
+              cja[cbase + slot] = col;
+              nslots++;
+            } else {
+              t.vals[slot] = xadd(t.vals[slot], v);
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+  nslots = __shfl_sync(0xffffffffu, nslots, 0);
+  for (int q = lane; q < nslots; q += 32) cval[cbase + q] = t.vals[q];
+  __syncwarp();
+}
+
+// ---------------- pass 1 kernels
+// class 0: per-warp shared table; class 1: one warp per block, big table;
+// class 2: global table (toff gives each listed row's table offset)
+__global__ void __launch_bounds__(32 * kRapWarps)
+k_rap_count_warp(const int* __restrict__ ria, const int* __restrict__ rja,
+                 const int* __restrict__ aia, const int* __restrict__ aja,
+                 const int* __restrict__ pia, const int* __restrict__ pja,
+                 const int* __restrict__ rows, int m, int* __restrict__ cnt_out) {
+  __shared__ int keys_s[kRapWarps][kWarpCap];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Table t{keys_s[w], nullptr, nullptr, kWarpCap - 1};
+  for (int q = blockIdx.x * kRapWarps + w; q < m; q += gridDim.x * kRapWarps) {
+    const int ic = rows[q];
+    int c = rap_count_row(ic, t, lane, ria, rja, aia, aja, pia, pja);
+    if (lane == 0) cnt_out[ic] = c;
+  }
+}
+
+__global__ void __launch_bounds__(32)
+k_rap_count_big(const int* __restrict__ ria, const int* __restrict__ rja,
+                const int* __restrict__ aia, const int* __restrict__ aja,
+                const int* __restrict__ pia, const int* __restrict__ pja,
+                const int* __restrict__ rows, int m, int* __restrict__ cnt_out) {
+  extern __shared__ int dyn[];
+  const int lane = threadIdx.x & 31;
+  Table t{dyn, nullptr, nullptr, kBigCap - 1};
+  for (int q = blockIdx.x; q < m; q += gridDim.x) {
+    const int ic = rows[q];
+    int c = rap_count_row(ic, t, lane, ria, rja, aia, aja, pia, pja);
+    if (lane == 0) cnt_out[ic] = c;
+  }
+}
+
+__global__ void k_rap_count_huge(const int* __restrict__ ria, const int* __restrict__ rja,
+                                 const int* __restrict__ aia, const int* __restrict__ aja,
+                                 const int* __restrict__ pia, const int* __restrict__ pja,
+                                 const int* __restrict__ rows, int m,
+                                 const long long* __restrict__ toff, int* __restrict__ gkeys,
+                                 int* __restrict__ cnt_out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += warps) {
+    const int ic = rows[q];
+    const long long off = toff[q];
+    Table t{gkeys + off, nullptr, nullptr, (unsigned)(toff[q + 1] - off) - 1};
+    int c = rap_count_row(ic, t, lane, ria, rja, aia, aja, pia, pja);
+    if (lane == 0) cnt_out[ic] = c;
+  }
+}
+
+// ---------------- pass 2 kernels
+constexpr size_t kWarpFillSmem =
+    kRapWarps * (kWarpCap * 2 * sizeof(int) + (kWarpCap / 2) * sizeof(double) +
+                 kBuf * (sizeof(int) + sizeof(double)));
+constexpr size_t kBigFillSmem =
+    kBigCap * 2 * sizeof(int) + (kBigCap / 2) * sizeof(double) + kBuf * (sizeof(int) + sizeof(double));
+constexpr size_t kBigCountSmem = kBigCap * sizeof(int);
+
+__device__ __forceinline__ void carve(unsigned char* base, int cap, Table* t, int** bcol,
+                                      double** bval) {
+  double* vals = (double*)base;                       // cap/2 doubles
+  double* bv = vals + cap / 2;                        // kBuf doubles
+  int* keys = (int*)(bv + kBuf);                      // cap ints
+  int* slots = keys + cap;                            // cap ints
+  int* bc = slots + cap;                              // kBuf ints
+  *t = Table{keys, slots, vals, (unsigned)cap - 1};
+  *bcol = bc;
+  *bval = bv;
+}
+
+__global__ void __launch_bounds__(32 * kRapWarps)
+k_rap_fill_warp(const int* __restrict__ ria, const int* __restrict__ rja,
+                const double* __restrict__ rval, const int* __restrict__ aia,
+                const int* __restrict__ aja, const double* __restrict__ aval,
+                const int* __restrict__ pia, const int* __restrict__ pja,
+                const double* __restrict__ pval, const int* __restrict__ rows, int m,
+                const int* __restrict__ cia, int* __restrict__ cja, double* __restrict__ cval) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Table t;
+  int* bcol;
+  double* bval;
+  carve(smem + w * (kWarpFillSmem / kRapWarps), kWarpCap, &t, &bcol, &bval);
+  for (int q = blockIdx.x * kRapWarps + w; q < m; q += gridDim.x * kRapWarps) {
+    const int ic = rows[q];
+    rap_fill_row(ic, t, lane, bcol, bval, ria, rja, rval, aia, aja, aval, pia, pja, pval, cia[ic],
+                 cja, cval);
+  }
+}
+
+__global__ void __launch_bounds__(32)
+k_rap_fill_big(const int* __restrict__ ria, const int* __restrict__ rja,
+               const double* __restrict__ rval, const int* __restrict__ aia,
+               const int* __restrict__ aja, const double* __restrict__ aval,
+               const int* __restrict__ pia, const int* __restrict__ pja,
+               const double* __restrict__ pval, const int* __restrict__ rows, int m,
+               const int* __restrict__ cia, int* __restrict__ cja, double* __restrict__ cval) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  Table t;
+  int* bcol;
+  double* bval;
+  carve(smem, kBigCap, &t, &bcol, &bval);
+  for (int q = blockIdx.x; q < m; q += gridDim.x) {
+    const int ic = rows[q];
+    rap_fill_row(ic, t, lane, bcol, bval, ria, rja, rval, aia, aja, aval, pia, pja, pval, cia[ic],
+                 cja, cval);
+  }
+}
+
+__global__ void k_rap_fill_huge(const int* __restrict__ ria, const int* __restrict__ rja,
+                                const double* __restrict__ rval, const int* __restrict__ aia,
+                                const int* __restrict__ aja, const double* __restrict__ aval,
+                                const int* __restrict__ pia, const int* __restrict__ pja,
+                                const double* __restrict__ pval, const int* __restrict__ rows,
+                                int m, const long long* __restrict__ toff,
+                                int* __restrict__ gkeys, int* __restrict__ gslots,
+                                double* __restrict__ gvals, int* __restrict__ gbcol,
+                                double* __restrict__ gbval, const int* __restrict__ cia,
+                                int* __restrict__ cja, double* __restrict__ cval) {
+  const int lane = threadIdx.x & 31;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  int* bcol = gbcol + (size_t)wid * kBuf;
+  double* bval = gbval + (size_t)wid * kBuf;
+  for (int q = wid; q < m; q += warps) {
+    const int ic = rows[q];
+    const long long off = toff[q];
+    const unsigned cap = (unsigned)(toff[q + 1] - off);
+    Table t{gkeys + off, gslots + off, gvals + off / 2, cap - 1};
+    rap_fill_row(ic, t, lane, bcol, bval, ria, rja, rval, aia, aja, aval, pia, pja, pval, cia[ic],
+                 cja, cval);
+  }
+}
+
+// ---------------- hub rows: sort-based fill
+// For rows with more than kSortProducts products the single-lane consumer
+// above would serialise too much work.  Their ordered product streams are
+// written out in full -- a (column, 0.0) seed for the diagonal first, then
+// every (r*a)*p in the reference's order -- sorted stably by (row, column),
+// so the products of one column stay in stream order; one thread per column
+// then sums them in that order (the first product assigned, the rest added,
+// exactly as the reference), and the columns are put back in order of first
+// appearance, which places the diagonal first.
+constexpr long long kSortProducts = 16384;
+
+__global__ void k_rap_gen_stream(const int* __restrict__ ria, const int* __restrict__ rja,
+                                 const double* __restrict__ rval, const int* __restrict__ aia,
+                                 const int* __restrict__ aja, const double* __restrict__ aval,
+                                 const int* __restrict__ pia, const int* __restrict__ pja,
+                                 const double* __restrict__ pval, const int* __restrict__ rows,
+                                 int m, const long long* __restrict__ poff,
+                                 unsigned long long* __restrict__ keys,
+                                 long long* __restrict__ idx, double* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += warps) {
+    const int ic = rows[q];
+    const unsigned long long hi = (unsigned long long)q << 32;
+    long long pos = poff[q];
+    if (lane == 0) {
+      keys[pos] = hi | (unsigned)ic;
+      idx[pos] = pos;
+      vals[pos] = 0.0;
+    }
+    pos++;
+    for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
+      const double r = rval[k1];
+      const int i1 = rja[k1];
+      const int a1 = aia[i1 + 1];
+      for (int base = aia[i1]; base < a1; base += 32) {
+        const int k2 = base + lane;
+        double ra = 0.0;
+        int p0 = 0, plen = 0;
+        if (k2 < a1) {
+          ra = xmul(r, aval[k2]);
+          const int i2 = aja[k2];
+          p0 = pia[i2];
+          plen = pia[i2 + 1] - p0;
+        }
+        int incl = plen;
+        for (int off = 1; off < 32; off <<= 1) {
+          int v = __shfl_up_sync(0xffffffffu, incl, off);
+          if (lane >= off) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const long long o = pos + incl - plen;
+        for (int q3 = 0; q3 < plen; q3++) {
+          keys[o + q3] = hi | (unsigned)pja[p0 + q3];
+          idx[o + q3] = o + q3;
+          vals[o + q3] = xmul(ra, pval[p0 + q3]);
+        }
+        pos += total;
+      }
+    }
+  }
+}
+
+__global__ void k_seg_heads(const unsigned long long* __restrict__ keys, long long T,
+                            unsigned char* __restrict__ head) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < T;
+       p += (long long)gridDim.x * blockDim.x)
+    head[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1 : 0;
+}
+
+__global__ void k_iota64(long long* __restrict__ a, long long T) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < T;
+       p += (long long)gridDim.x * blockDim.x)
+    a[p] = p;
+}
+
+// one thread per column segment: ordered sum; key for reordering = first
+// stream position of the column
+__global__ void k_seg_sum(const unsigned long long* __restrict__ keys,
+                          const long long* __restrict__ idx, const double* __restrict__ vals,
+                          const long long* __restrict__ seg, long long nseg, long long T,
+                          double* __restrict__ sval, int* __restrict__ scol,
+                          long long* __restrict__ sfirst) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long b = seg[g], e = (g + 1 < nseg) ? seg[g + 1] : T;
+    double v = vals[idx[b]];
+    for (long long p = b + 1; p < e; p++) v = xadd(v, vals[idx[p]]);
+    sval[g] = v;
+    scol[g] = (int)(keys[b] & 0xffffffffull);
+    sfirst[g] = idx[b];
+  }
+}
+
+// write the reordered columns of each hub row
+__global__ void k_seg_write(const long long* __restrict__ order, long long nseg,
+                            const unsigned long long* __restrict__ seg_key_row,
+                            const double* __restrict__ sval, const int* __restrict__ scol,
+                            const int* __restrict__ rows, const long long* __restrict__ rowseg,
+                            const int* __restrict__ cia, int* __restrict__ cja,
+                            double* __restrict__ cval) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nseg;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long g = order[t];
+    const int q = (int)(seg_key_row[g] >> 32);
+    const int ic = rows[q];
+    const long long rank = t - rowseg[q];
+    cja[cia[ic] + rank] = scol[g];
+    cval[cia[ic] + rank] = sval[g];
+  }
+}
+
+__global__ void k_seg_rowkeys(const unsigned long long* __restrict__ keys,
+                              const long long* __restrict__ seg, long long nseg,
+                              unsigned long long* __restrict__ out) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
+       g += (long long)gridDim.x * blockDim.x)
+    out[g] = keys[seg[g]];
+}
+
+__global__ void k_rows_count64(const int* __restrict__ rows, int m, const long long* __restrict__ v,
+                               long long sub, long long* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    out[q] = v[rows[q]] - sub;
+}
+
+static void rap_fill_sorted(const CSR& R, const CSR& A, const CSR& P, const int* rows, int m,
+                            const long long* ub, const long long* exact, CSR& Ac,
+                            cudaStream_t s) {
+  // product offsets (ub counts the diagonal seed)
+  DBuf<long long> poff((size_t)m + 1, s), rowseg((size_t)m + 1, s);
+  poff.zero();
+  rowseg.zero();
+  BN_LAUNCH(k_rows_count64, grid_for(m, 128), 128, 0, s, rows, m, ub, 0LL, poff.p);
+  const long long T = scan_counts64(poff.p, m, s);
+  BN_LAUNCH(k_rows_count64, grid_for(m, 128), 128, 0, s, rows, m, exact, 0LL, rowseg.p);
+  const long long nseg_expect = scan_counts64(rowseg.p, m, s);
+  DBuf<unsigned long long> keys(T, s), keys2(T, s);
+  DBuf<long long> idx(T, s), idx2(T, s);
+  DBuf<double> vals(T, s);
+  BN_LAUNCH(k_rap_gen_stream, grid_for((long long)m * 32, 128), 128, 0, s, R.ia.p, R.ja.p,
+            R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, rows, m, poff.p, keys.p,
+            idx.p, vals.p);
+  int eb = 33;
+  while ((1LL << (eb - 32)) < (long long)m) eb++;
+  size_t tmp = 0;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, idx2.p, T, 0, eb,
+                                          s));
+  DBuf<unsigned char> tb(tmp, s);
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, keys.p, keys2.p, idx.p, idx2.p, T, 0, eb, s));
+  // segment heads -> segment starts
+  DBuf<unsigned char> head(T, s);
+  DBuf<long long> iota(T, s), seg(T, s), nsel(1, s);
+  BN_LAUNCH(k_seg_heads, grid_for(T, 256), 256, 0, s, keys2.p, T, head.p);
+  BN_LAUNCH(k_iota64, grid_for(T, 256), 256, 0, s, iota.p, T);
+  tmp = 0;
+  BN_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, iota.p, head.p, seg.p, nsel.p, T, s));
+  DBuf<unsigned char> tb2(tmp, s);
+  BN_CUDA(cub::DeviceSelect::Flagged(tb2.p, tmp, iota.p, head.p, seg.p, nsel.p, T, s));
+  const long long nseg = read_scalar(nsel.p, s);
+  BN_REQUIRE(nseg == nseg_expect, BN_ERR_ARG, "RAP: hub-row column count mismatch");
+  DBuf<double> sval(nseg, s);
+  DBuf<int> scol(nseg, s);
+  DBuf<long long> sfirst(nseg, s), sfirst2(nseg, s), g_in(nseg, s), g_out(nseg, s);
+  DBuf<unsigned long long> srow(nseg, s);
+  BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, keys2.p, idx2.p, vals.p, seg.p, nseg, T,
+            sval.p, scol.p, sfirst.p);
+  BN_LAUNCH(k_seg_rowkeys, grid_for(nseg, 256), 256, 0, s, keys2.p, seg.p, nseg, srow.p);
+  // order the columns of every row by first stream position (rows stay in
+  // order because their stream ranges are increasing)
+  BN_LAUNCH(k_iota64, grid_for(nseg, 256), 256, 0, s, g_in.p, nseg);
+  int fb = 1;
+  while ((1LL << fb) <= T) fb++;
+  tmp = 0;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, sfirst.p, sfirst2.p, g_in.p, g_out.p, nseg,
+                                          0, fb, s));
+  DBuf<unsigned char> tb3(tmp, s);
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(tb3.p, tmp, sfirst.p, sfirst2.p, g_in.p, g_out.p, nseg,
+                                          0, fb, s));
+  BN_LAUNCH(k_seg_write, grid_for(nseg, 256), 256, 0, s, g_out.p, nseg, srow.p, sval.p, scol.p,
+            rows, rowseg.p, Ac.ia.p, Ac.ja.p, Ac.val.p);
+}
+
+// ---------------- classification helpers
+// class by a size estimate: 0 (<= kWarpCap/2), 1 (<= kBigCap/2), 2 (beyond)
+__global__ void k_rap_classify(const long long* __restrict__ est, int nc, int cap_limit,
+                               int* __restrict__ lists, int* __restrict__ counts) {
+  for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+    long long e = est[ic];
+    if (e < 0) continue;  // handled elsewhere
+    if (e > cap_limit) e = cap_limit;
+    int c = e <= kWarpCap / 2 ? 0 : (e <= kBigCap / 2 ? 1 : 2);
+    int pos = atomicAdd(&counts[c], 1);
+    lists[(size_t)c * nc + pos] = ic;
+  }
+}
+
+__global__ void k_rap_split_hubs(const long long* __restrict__ ub,
+                                 const long long* __restrict__ exact, int nc,
+                                 long long* __restrict__ est, int* __restrict__ hub, int* nh) {
+  for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
+    if (ub[ic] > kSortProducts) {
+      est[ic] = -1;
+      hub[atomicAdd(nh, 1)] = ic;
+    } else {
+      est[ic] = exact[ic];
+    }
+  }
+}
+
+__global__ void k_rap_huge_caps(const long long* __restrict__ est, const int* __restrict__ rows,
+                                int m, int cap_limit, long long* __restrict__ cap) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+    long long need = est[rows[q]];
+    if (need > cap_limit) need = cap_limit;
+    need *= 2;
+    long long c = 64;
+    while (c < need) c <<= 1;
+    cap[q] = c;
+  }
+}
+
+__global__ void k_i32_to_i64(const int* __restrict__ a, int n, long long* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = a[i];
+}
+
+struct RapClasses {
+  DBuf<int> lists;  // 3 x nc
+  int count[3] = {0, 0, 0};
+};
+
+static void classify(const long long* est, int nc, RapClasses& rc, cudaStream_t s) {
+  rc.lists.alloc((size_t)3 * (nc > 0 ? nc : 1), s);
+  DBuf<int> cnt(3, s);
+  cnt.zero();
+  if (nc > 0)
+    BN_LAUNCH(k_rap_classify, grid_for(nc, 256), 256, 0, s, est, nc, nc, rc.lists.p, cnt.p);
+  cnt.download(rc.count, 3);
+  BN_CUDA(cudaStreamSynchronize(s));
+}
+
+void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
+  const int nc = R.n;
+  {
+    BN_CUDA(cudaFuncSetAttribute(k_rap_fill_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kWarpFillSmem));
+    BN_CUDA(cudaFuncSetAttribute(k_rap_fill_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kBigFillSmem));
+    BN_CUDA(cudaFuncSetAttribute(k_rap_count_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kBigCountSmem));
+  }
+  DBuf<long long> ub(nc > 0 ? nc : 1, s);
+  DBuf<int> cnt((size_t)nc + 1, s);
+  cnt.zero();
+  if (nc > 0)
+    BN_LAUNCH(k_rap_bound, grid_for((long long)nc * 32, 256, 16), 256, 0, s, R.ia.p, R.ja.p,
+              A.ia.p, A.ja.p, P.ia.p, nc, ub.p);
+  // ---- pass 1: count, classified by min(bound, nc)
+  {
+    RapClasses rc;
+    classify(ub.p, nc, rc, s);
+    const int* L0 = rc.lists.p;
+    const int* L1 = rc.lists.p + nc;
+    const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    if (rc.count[0])
+      BN_LAUNCH(k_rap_count_warp, grid_for(rc.count[0], kRapWarps, 64), 32 * kRapWarps, 0, s,
+                R.ia.p, R.ja.p, A.ia.p, A.ja.p, P.ia.p, P.ja.p, L0, rc.count[0], cnt.p);
+    if (rc.count[1])
+      BN_LAUNCH(k_rap_count_big, grid_for(rc.count[1], 1, 16), 32, kBigCountSmem, s, R.ia.p,
+                R.ja.p, A.ia.p, A.ja.p, P.ia.p, P.ja.p, L1, rc.count[1], cnt.p);
+    if (rc.count[2]) {
+      const int m = rc.count[2];
+      DBuf<long long> toff((size_t)m + 1, s);
+      toff.zero();
+      BN_LAUNCH(k_rap_huge_caps, grid_for(m, 128), 128, 0, s, ub.p, L2, m, nc, toff.p);
+      long long total = scan_counts64(toff.p, m, s);
+      DBuf<int> gkeys((size_t)total, s);
+      BN_LAUNCH(k_rap_count_huge, grid_for((long long)m * 32, 128), 128, 0, s, R.ia.p, R.ja.p,
+                A.ia.p, A.ja.p, P.ia.p, P.ja.p, L2, m, toff.p, gkeys.p, cnt.p);
+    }
+  }
+  // exact per-row counts (before the scan) drive the fill classes
+  DBuf<long long> exact(nc > 0 ? nc : 1, s);
+  if (nc > 0) BN_LAUNCH(k_i32_to_i64, grid_for(nc, 256), 256, 0, s, cnt.p, nc, exact.p);
+  int nnz = scan_counts(cnt.p, nc, s);
+  Ac.n = nc;
+  Ac.m = P.m;
+  Ac.nnz = nnz;
+  Ac.ia = std::move(cnt);
+  Ac.ja.alloc((size_t)(nnz > 0 ? nnz : 1), s);
+  Ac.val.alloc((size_t)(nnz > 0 ? nnz : 1), s);
+  // ---- pass 2: fill (hub rows by the sort path, the rest by lane-0 streams)
+  {
+    DBuf<long long> est(nc > 0 ? nc : 1, s);
+    DBuf<int> hub(nc > 0 ? nc : 1, s), nh(1, s);
+    nh.zero();
+    if (nc > 0)
+      BN_LAUNCH(k_rap_split_hubs, grid_for(nc, 256), 256, 0, s, ub.p, exact.p, nc, est.p, hub.p,
+                nh.p);
+    const int nhub = read_scalar(nh.p, s);
+    if (nhub > 0) rap_fill_sorted(R, A, P, hub.p, nhub, ub.p, exact.p, Ac, s);
+    RapClasses rc;
+    classify(est.p, nc, rc, s);
+    const int* L0 = rc.lists.p;
+    const int* L1 = rc.lists.p + nc;
+    const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    if (rc.count[0])
+      BN_LAUNCH(k_rap_fill_warp, grid_for(rc.count[0], kRapWarps, 32), 32 * kRapWarps,
+                kWarpFillSmem, s, R.ia.p, R.ja.p, R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p,
+                P.ja.p, P.val.p, L0, rc.count[0], Ac.ia.p, Ac.ja.p, Ac.val.p);
+    if (rc.count[1])
+      BN_LAUNCH(k_rap_fill_big, grid_for(rc.count[1], 1, 2), 32, kBigFillSmem, s, R.ia.p, R.ja.p,
+                R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, L1, rc.count[1],
+                Ac.ia.p, Ac.ja.p, Ac.val.p);
+    if (rc.count[2]) {
+      const int m = rc.count[2];
+      DBuf<long long> toff((size_t)m + 1, s);
+      toff.zero();
+      BN_LAUNCH(k_rap_huge_caps, grid_for(m, 128), 128, 0, s, exact.p, L2, m, nc, toff.p);
+      long long total = scan_counts64(toff.p, m, s);
+      const int grid = grid_for((long long)m * 32, 128);
+      const size_t nwarps = (size_t)grid * 4;
+      DBuf<int> gkeys((size_t)total, s), gslots((size_t)total, s), gbcol(nwarps * kBuf, s);
+      DBuf<double> gvals((size_t)total / 2 + 1, s), gbval(nwarps * kBuf, s);
+      BN_LAUNCH(k_rap_fill_huge, grid, 128, 0, s, R.ia.p, R.ja.p, R.val.p, A.ia.p, A.ja.p,
+                A.val.p, P.ia.p, P.ja.p, P.val.p, L2, m, toff.p, gkeys.p, gslots.p, gvals.p,
+                gbcol.p, gbval.p, Ac.ia.p, Ac.ja.p, Ac.val.p);
+    }
+  }
+}
+
+}  // namespace bn

@@ -1,0 +1,327 @@
+// Solve-phase kernels: CSR SpMV family, coloured Gauss-Seidel, PCG vector
+// updates with fused reductions.  Templated on the value type: float64 for
+// the plain solver and the outer PCG, float32 (with float32 accumulation)
+// for the mixed-precision V-cycle.
+//
+// SpMV layout ("CSR-stream"): a block of kRows rows loads the contiguous
+// nonzero range of its rows with coalesced loads, forms the products
+// a_ij * x_j into shared memory, then each thread sums its own row in
+// storage order -- the reference's summation order for abyvg/abyvam/abyvcs
+// (C_amg1/src/sparse_ops.c:19-56), with separate multiply and add.  Tiles
+// whose nonzeros exceed the shared buffer fall back to a per-thread walk.
+#include "solve_kernels.cuh"
+
+namespace bn {
+
+template <class T> __device__ __forceinline__ T dmul(T a, T b);
+template <> __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+template <> __device__ __forceinline__ float dmul(float a, float b) { return __fmul_rn(a, b); }
+template <class T> __device__ __forceinline__ T dadd(T a, T b);
+template <> __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+template <> __device__ __forceinline__ float dadd(float a, float b) { return __fadd_rn(a, b); }
+template <class T> __device__ __forceinline__ T dsub(T a, T b);
+template <> __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+template <> __device__ __forceinline__ float dsub(float a, float b) { return __fsub_rn(a, b); }
+
+// -------------------------------------------------------------------- SpMV
+template <class T, int MODE, bool DOT>
+__global__ void __launch_bounds__(kRows)
+k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+       const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
+       const T* __restrict__ dw, double* __restrict__ partial) {
+  __shared__ T prod[kTileNnz];
+  __shared__ double red[kRows / 32];
+  double dot = 0.0;
+  for (int r0 = blockIdx.x * kRows; r0 < n; r0 += gridDim.x * kRows) {
+    const int r1 = min(r0 + kRows, n);
+    const int e0 = ia[r0], e1 = ia[r1];
+    const int i = r0 + threadIdx.x;
+    T hold = T(0);
+    if (e1 - e0 <= kTileNnz) {
+      for (int k = e0 + threadIdx.x; k < e1; k += kRows) prod[k - e0] = dmul(a[k], x[ja[k]]);
+      __syncthreads();
+      if (i < r1) {
+        if (MODE == SPMV_RES) hold = b[i];
+        if (MODE == SPMV_ADD) hold = y[i];
+        const int k0 = ia[i] - e0, k1 = ia[i + 1] - e0;
+        for (int k = k0; k < k1; k++)
+          hold = (MODE == SPMV_RES) ? dsub(hold, prod[k]) : dadd(hold, prod[k]);
+      }
+      __syncthreads();
+    } else if (i < r1) {
+      if (MODE == SPMV_RES) hold = b[i];
+      if (MODE == SPMV_ADD) hold = y[i];
+      for (int k = ia[i]; k < ia[i + 1]; k++) {
+        T p = dmul(a[k], x[ja[k]]);
+        hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
+      }
+    }
+    if (i < r1) {
+      y[i] = hold;
+      if (DOT) dot += (double)dw[i] * (double)hold;
+    }
+  }
+  if (DOT) {
+    for (int off = 16; off > 0; off >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kRows / 32; w++) t += red[w];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+template <class T>
+void spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
+          const T* dot_w, double* partial) {
+  if (A.n == 0) return;
+  int grid = spmv_grid(A.n);
+  if (dot_w) {
+    BN_LAUNCH((k_spmv<T, SPMV_Y, true>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dot_w,
+              partial);
+    return;
+  }
+  switch (mode) {
+    case SPMV_Y:
+      BN_LAUNCH((k_spmv<T, SPMV_Y, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                nullptr, nullptr);
+      break;
+    case SPMV_RES:
+      BN_LAUNCH((k_spmv<T, SPMV_RES, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                nullptr, nullptr);
+      break;
+    default:
+      BN_LAUNCH((k_spmv<T, SPMV_ADD, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                nullptr, nullptr);
+      break;
+  }
+}
+
+// ----------------------------------------------------- coloured Gauss-Seidel
+// x_i = (b_i - sum_{j != i} a_ij x_j) / a_ii for the rows of one colour
+// (cf_fwd_gs / cf_bwd_gs, C_amg1/src/amg_cycle.c:52-80; diagonal 1.0 if
+// missing).  Rows of one colour share no edge, so a colour is one launch.
+// G lanes per row (1 for the short rows of fine levels, 8 or 32 for the
+// denser coarse operators).  OUT == nullptr updates x in place; otherwise the
+// new values go to out[t] (Jacobi-style overflow classes whose rows may be
+// adjacent are computed into a buffer first, then scattered).
+template <class T, int G>
+__global__ void k_gs_color(const int* __restrict__ ia, const int* __restrict__ ja,
+                           const T* __restrict__ a, const int* __restrict__ rows, int nr,
+                           const T* __restrict__ b, T* x, T* __restrict__ out) {
+  const int gl = threadIdx.x & (G - 1);
+  const int groups = (gridDim.x * blockDim.x) / G;
+  unsigned gmask = 0xffffffffu;
+  if constexpr (G < 32) gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) / G; t < nr; t += groups) {
+    const int i = rows[t];
+    T sum = T(0), d = T(0);
+    bool has_d = false;
+    for (int k = ia[i] + gl; k < ia[i + 1]; k += G) {
+      const int j = ja[k];
+      const T v = a[k];
+      if (j == i) { d = v; has_d = true; }
+      else sum = dadd(sum, dmul(v, x[j]));
+    }
+    if (G > 1) {
+#pragma unroll
+      for (int off = G / 2; off > 0; off >>= 1) {
+        sum = dadd(sum, __shfl_xor_sync(gmask, sum, off, G));
+        T od = __shfl_xor_sync(gmask, d, off, G);
+        bool oh = __shfl_xor_sync(gmask, has_d, off, G);
+        if (oh) { d = od; has_d = true; }
+      }
+    }
+    if (gl == 0) {
+      const T xi = dsub(b[i], sum) / (has_d ? d : T(1));
+      if (out) out[t] = xi; else x[i] = xi;
+    }
+  }
+}
+
+template <class T>
+__global__ void k_scatter(const int* __restrict__ rows, int nr, const T* __restrict__ v,
+                          T* __restrict__ x) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x)
+    x[rows[t]] = v[t];
+}
+
+template <class T>
+static void gs_launch(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* out,
+                      int group, cudaStream_t s) {
+  if (group >= 32)
+    BN_LAUNCH((k_gs_color<T, 32>), grid_for((long long)nr * 32, 256, 8), 256, 0, s, A.ia, A.ja,
+              A.val, rows, nr, b, x, out);
+  else if (group >= 8)
+    BN_LAUNCH((k_gs_color<T, 8>), grid_for((long long)nr * 8, 256, 8), 256, 0, s, A.ia, A.ja,
+              A.val, rows, nr, b, x, out);
+  else
+    BN_LAUNCH((k_gs_color<T, 1>), grid_for(nr, 128, 16), 128, 0, s, A.ia, A.ja, A.val, rows, nr,
+              b, x, out);
+}
+
+template <class T>
+void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
+              cudaStream_t s) {
+  if (nr == 0) return;
+  gs_launch<T>(A, rows, nr, b, x, nullptr, group, s);
+}
+
+template <class T>
+void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
+                  int group, cudaStream_t s) {
+  if (nr == 0) return;
+  gs_launch<T>(A, rows, nr, b, x, tmp, group, s);
+  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, nr, tmp, x);
+}
+
+// ------------------------------------------------------------ vector ops
+template <class T>
+__global__ void k_zero(T* __restrict__ x, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = T(0);
+}
+template <class T>
+void vzero(T* x, int n, cudaStream_t s) {
+  if (n) BN_LAUNCH(k_zero<T>, grid_for(n, 256), 256, 0, s, x, n);
+}
+
+template <class TO, class TI>
+__global__ void k_convert(const TI* __restrict__ a, int n, TO* __restrict__ b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = (TO)a[i];
+}
+template <class TO, class TI>
+void vconvert(const TI* a, int n, TO* b, cudaStream_t s) {
+  if (n) BN_LAUNCH((k_convert<TO, TI>), grid_for(n, 256), 256, 0, s, a, n, b);
+}
+
+// x = u + v  (x may alias u)
+template <class T>
+__global__ void k_add(const T* __restrict__ u, const T* __restrict__ v, int n, T* x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = dadd(u[i], v[i]);
+}
+template <class T>
+void vadd(const T* u, const T* v, int n, T* x, cudaStream_t s) {
+  if (n) BN_LAUNCH(k_add<T>, grid_for(n, 256), 256, 0, s, u, v, n, x);
+}
+
+// block partial sums -> one scalar (deterministic order)
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+  return t;
+}
+
+template <class T>
+__global__ void k_dot2(const T* __restrict__ u, const T* __restrict__ v,
+                       const T* __restrict__ w, int n, double* __restrict__ p0,
+                       double* __restrict__ p1) {
+  __shared__ double red[32];
+  double a = 0.0, c = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double ui = (double)u[i];
+    a += ui * (double)v[i];
+    if (w) c += ui * (double)w[i];
+  }
+  double ta = block_sum(a, red);
+  __syncthreads();
+  double tc = w ? block_sum(c, red) : 0.0;
+  if (threadIdx.x == 0) {
+    p0[blockIdx.x] = ta;
+    if (w) p1[blockIdx.x] = tc;
+  }
+}
+
+// u.v (and u.w) into partial arrays of kRedBlocks entries
+template <class T>
+void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double* p1,
+                  cudaStream_t s) {
+  BN_LAUNCH(k_dot2<T>, kRedBlocks, 256, 0, s, u, v, w, n, p0, p1);
+}
+
+// Reduce a partial array into slot `dst` of the scalar block.
+__global__ void k_reduce(const double* __restrict__ part, int m, double* __restrict__ out) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) v += part[i];
+  double t = block_sum(v, red);
+  if (threadIdx.x == 0) *out = t;
+}
+void reduce_partials(const double* part, int m, double* out, cudaStream_t s) {
+  BN_LAUNCH(k_reduce, 1, 1024, 0, s, part, m, out);
+}
+
+// x += alpha p ; r -= alpha Ap ; partial r.r     (alpha = sc[RZ] / sc[PAP])
+__global__ void k_pcg_update_xr(double* __restrict__ x, double* __restrict__ r,
+                                const double* __restrict__ p, const double* __restrict__ ap,
+                                int n, const double* __restrict__ sc, double* __restrict__ part) {
+  __shared__ double red[32];
+  const double alpha = sc[SC_RZ] / sc[SC_PAP];
+  double rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = x[i] + p[i] * alpha;        // uuplmv: u + v * smult
+    double ri = r[i] + ap[i] * (-alpha);
+    r[i] = ri;
+    rr += ri * ri;
+  }
+  double t = block_sum(rr, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
+                   const double* sc, double* part, cudaStream_t s) {
+  BN_LAUNCH(k_pcg_update_xr, kRedBlocks, 256, 0, s, x, r, p, ap, n, sc, part);
+}
+
+// p = z + beta p ; beta from the scalar block (standard or flexible)
+__global__ void k_pcg_update_p(double* __restrict__ p, const double* __restrict__ z, int n,
+                               const double* __restrict__ sc) {
+  const double beta = sc[SC_BETA];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = beta * p[i] + z[i];         // umuplv: smult * u + v
+}
+void pcg_update_p(double* p, const double* z, int n, const double* sc, cudaStream_t s) {
+  BN_LAUNCH(k_pcg_update_p, grid_for(n, 256), 256, 0, s, p, z, n, sc);
+}
+
+// After z = M r: reduce r.z (and r.z_old), form beta, rotate rz, publish the
+// convergence scalars.  One thread.
+__global__ void k_pcg_scalars(double* sc, int flexible) {
+  const double rz_new = sc[SC_RZNEW];
+  double beta;
+  if (flexible)
+    beta = (rz_new - sc[SC_RZOLD_NEW]) / sc[SC_RZ];  // r_{k+1}.(z_{k+1}-z_k) / r_k.z_k
+  else
+    beta = rz_new / sc[SC_RZ];
+  sc[SC_BETA] = beta;
+  sc[SC_RZ_PREV] = sc[SC_RZ];
+  sc[SC_RZ] = rz_new;
+}
+void pcg_scalars(double* sc, int flexible, cudaStream_t s) {
+  BN_LAUNCH(k_pcg_scalars, 1, 1, 0, s, sc, flexible);
+}
+
+// explicit instantiations
+#define BN_INST(T)                                                                           \
+  template void spmv<T>(int, const DevMat<T>&, const T*, const T*, T*, cudaStream_t, const T*, \
+                        double*);                                                            \
+  template void gs_color<T>(const DevMat<T>&, const int*, int, const T*, T*, int,            \
+                            cudaStream_t);                                                   \
+  template void jacobi_class<T>(const DevMat<T>&, const int*, int, const T*, T*, T*, int,     \
+                                cudaStream_t);                                               \
+  template void vzero<T>(T*, int, cudaStream_t);                                             \
+  template void vadd<T>(const T*, const T*, int, T*, cudaStream_t);                          \
+  template void dot_partials<T>(const T*, const T*, const T*, int, double*, double*,          \
+                                cudaStream_t);
+BN_INST(double)
+BN_INST(float)
+template void vconvert<float, double>(const double*, int, float*, cudaStream_t);
+template void vconvert<double, float>(const float*, int, double*, cudaStream_t);
+
+}  // namespace bn

@@ -1,0 +1,66 @@
+// Solve-phase kernel interfaces.
+#pragma once
+#include "common.cuh"
+
+namespace bn {
+
+constexpr int kRows = 256;        // rows per SpMV tile (= threads per block)
+constexpr int kTileNnz = 2048;    // shared product buffer per tile
+constexpr int kRedBlocks = 1184;  // blocks for reductions (8 per SM)
+
+enum SpmvMode : int { SPMV_Y = 0, SPMV_RES = 1, SPMV_ADD = 2 };
+
+// PCG scalar block slots (device memory)
+enum ScalarSlot : int {
+  SC_RZ = 0,        // r_k . z_k
+  SC_PAP = 1,       // p . Ap
+  SC_RR = 2,        // r . r
+  SC_RZNEW = 3,     // r_{k+1} . z_{k+1}
+  SC_RZOLD_NEW = 4, // r_{k+1} . z_k  (flexible beta)
+  SC_BETA = 5,
+  SC_RZ_PREV = 6,
+  SC_RZ0 = 7,
+  SC_BB = 8,
+  SC_COUNT = 16
+};
+
+// Non-owning CSR view with values of type T.
+template <class T>
+struct DevMat {
+  int n = 0, m = 0, nnz = 0;
+  const int* ia = nullptr;
+  const int* ja = nullptr;
+  const T* val = nullptr;
+};
+
+inline int spmv_grid(int n) {
+  int tiles = (n + kRows - 1) / kRows;
+  int cap = kSMs * 8;
+  return tiles < cap ? tiles : cap;
+}
+
+template <class T>
+void spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
+          const T* dot_w = nullptr, double* partial = nullptr);
+template <class T>
+void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
+              cudaStream_t s);
+template <class T>
+void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
+                  int group, cudaStream_t s);
+template <class T>
+void vzero(T* x, int n, cudaStream_t s);
+template <class TO, class TI>
+void vconvert(const TI* a, int n, TO* b, cudaStream_t s);
+template <class T>
+void vadd(const T* u, const T* v, int n, T* x, cudaStream_t s);
+template <class T>
+void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double* p1,
+                  cudaStream_t s);
+void reduce_partials(const double* part, int m, double* out, cudaStream_t s);
+void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
+                   const double* sc, double* part, cudaStream_t s);
+void pcg_update_p(double* p, const double* z, int n, const double* sc, cudaStream_t s);
+void pcg_scalars(double* sc, int flexible, cudaStream_t s);
+
+}  // namespace bn

@@ -1,0 +1,984 @@
+// AMG-PCG solver on one B200: hierarchy setup, smoothers, the three-stage
+// AMG + IC(0) preconditioner, PCG, and the amg_solver_* C ABI.
+//
+// Reference call structure (C_amg1):
+//   amg_solver_create  amg_wrapper.c:51-97   copy, symmetrise, build, IC(0)
+//   amg_build_hierarchy build_hierarchy.c:29-156
+//   amg_ichol_precond  amg_ichol_precond.c:22-59
+//   backslash/fwdslash amg_cycle.c:180-253
+//   amg_pcg            amg_pcg.c:12-101
+// Setup kernels reproduce the reference bit for bit (strength, PMIS,
+// interpolation, RAP, symmetrisation, IC(0)); the solve phase uses a
+// multicolour Gauss-Seidel in place of the sequential CF-ordered sweep and a
+// dense direct coarse solve in place of the coarse PCG.
+#include "internal.cuh"
+#include "ichol.cuh"
+#include "dense.cuh"
+#include "solve_kernels.cuh"
+#include "../../include/amg_b200.h"
+
+#include <cub/cub.cuh>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <memory>
+
+namespace bn {
+
+// ------------------------------------------------------------ colouring
+__device__ __forceinline__ unsigned color_hash(unsigned x) {
+  // bijective 32-bit mix: distinct rows get distinct priorities
+  x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+  return x;
+}
+
+// Jones-Plassmann-Luby rounds with first-fit colours: an uncoloured row
+// whose priority beats every uncoloured neighbour of its own set takes the
+// smallest colour that no already-coloured neighbour of its set holds.
+// Rows selected in one round are never adjacent, so the colouring is
+// proper.  Colours are capped at kMaxColors per set; a row that finds all
+// of them taken joins the set's overflow class (colour kMaxColors), which the
+// smoother updates Jacobi-style.
+constexpr int kMaxColors = 32;
+
+__global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
+                              const int* __restrict__ set, int n, const int* __restrict__ color,
+                              int* __restrict__ newc, int* counter) {
+  int local = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    newc[i] = -1;
+    if (color[i] >= 0) continue;
+    const unsigned hi = color_hash((unsigned)i);
+    const int si = set ? set[i] : 0;
+    bool is_max = true;
+    unsigned used = 0;
+    for (int k = ia[i]; k < ia[i + 1]; k++) {
+      const int j = ja[k];
+      if (j == i) continue;
+      if (set && set[j] != si) continue;
+      const int cj = color[j];
+      if (cj >= 0) {
+        if (cj < kMaxColors) used |= 1u << cj;
+      } else if (color_hash((unsigned)j) > hi) {
+        is_max = false;
+        break;
+      }
+    }
+    if (is_max) {
+      newc[i] = (used == 0xffffffffu) ? kMaxColors : __ffs(~used) - 1;
+      local++;
+    }
+  }
+  if (local) atomicAdd(counter, local);
+}
+
+__global__ void k_color_commit(int n, const int* __restrict__ newc, int* __restrict__ color) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (newc[i] >= 0) color[i] = newc[i];
+}
+
+// key = set * 64 + colour ; C points are set 0, F points set 1
+__global__ void k_color_keys(const int* __restrict__ set, const int* __restrict__ color, int n,
+                             int* __restrict__ key, int* __restrict__ ids) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    key[i] = (set ? set[i] : 0) * 64 + color[i];
+    ids[i] = i;
+  }
+}
+
+__global__ void k_cf_set(const int* __restrict__ cf, int n, int* __restrict__ set) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    set[i] = (cf[i] == 1) ? 0 : 1;
+}
+
+__global__ void k_l1_diag(const int* __restrict__ ia, const double* __restrict__ a, int n,
+                          double* __restrict__ d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = ia[i]; k < ia[i + 1]; k++) s += fabs(a[k]);
+    d[i] = s;
+  }
+}
+
+__global__ void k_diag(const int* __restrict__ ia, const int* __restrict__ ja,
+                       const double* __restrict__ a, int n, double* __restrict__ d) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = 1.0;
+    for (int k = ia[i]; k < ia[i + 1]; k++)
+      if (ja[k] == i) v = a[k];
+    d[i] = v;
+  }
+}
+
+// x += w_i * r_i  with w_i = scale / d_i
+template <class T>
+__global__ void k_scaled_update(T* __restrict__ x, const T* __restrict__ r,
+                                const T* __restrict__ d, T scale, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] += scale * (r[i] / d[i]);
+}
+
+template <class T>
+__global__ void k_to_f32(const double* __restrict__ a, size_t m, T* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (T)a[i];
+}
+
+// ------------------------------------------------------------ data
+struct Level {
+  CSR A, S, P, R;
+  DBuf<int> cf;
+  int n_coarse = 0;
+  int max_lam = 0;
+  DBuf<float> A32, P32, R32;
+  // smoother colouring: rows grouped by (set, colour)
+  DBuf<int> gs_rows;
+  std::vector<int> cptr;   // colour class offsets into gs_rows
+  std::vector<char> cjac;  // class is an overflow class (Jacobi update)
+  int colored_for = -1;    // smoother the colouring was built for
+  int color_rounds = 0;
+  int gs_group = 1;        // lanes per row in the GS kernel
+  DBuf<double> l1, dg;
+  DBuf<float> l1_32, dg32;
+  // work vectors
+  DBuf<double> b, x, r;
+  DBuf<float> b32, x32, r32;
+};
+
+struct Solver {
+  int device = 0;
+  cudaStream_t s = 0;
+  amg_b200_options opt{};
+  std::vector<std::unique_ptr<Level>> lv;
+  DenseCoarse coarse;
+  CSR Aown;               // solve matrix when set_matrix replaced it
+  bool own_solve = false;
+  DBuf<float> Aown32;
+  IChol ic;
+  bool f32_ready = false;
+  // level-0 preconditioner vectors
+  DBuf<double> u1, r1, icy, icx, xx, r2, corr;
+  DBuf<float> g32, u1f, r1f, icyf, icxf, xxf, r2f, corrf;
+  // PCG vectors
+  DBuf<double> b, x, r, z, p, ap;
+  DBuf<double> sc, part0, part1;
+  double* h_sc = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  unsigned long long graph_kernels[2] = {0, 0};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  amg_solve_stats stats{};
+
+  ~Solver();
+  const CSR& Asolve() const { return own_solve ? Aown : lv[0]->A; }
+  int n() const { return Asolve().n; }
+  void build(CSR&& A0);
+  void rebuild_values(CSR&& A0);
+  void finish_setup();
+  void prepare_f32();
+  void color_level(Level& L, int smoother);
+  void alloc_vectors();
+  void drop_graphs();
+  template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32) const;
+  template <class T> void smooth(int l, const T* bb, T* xl, bool forward);
+  template <class T> void backslash(int l, const T* bb, T* xl);
+  template <class T> void fwdslash(int l, const T* bb, T* xl);
+  template <class T> void precond_t(const T* g, T* out);
+  void precond(const double* g, double* out);  // z = M g (FP64 interface)
+  int pcg(const double* d_b, double* d_x, double tol, int maxiter, int print_level);
+};
+
+Solver::~Solver() {
+  drop_graphs();
+  if (h_sc) cudaFreeHost(h_sc);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+}
+
+void Solver::drop_graphs() {
+  for (auto& g : graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+template <class T>
+DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32) const {
+  DevMat<T> d;
+  d.n = M.n; d.m = M.m; d.nnz = M.nnz; d.ia = M.ia.p; d.ja = M.ja.p;
+  if constexpr (sizeof(T) == 8) d.val = M.val.p;
+  else d.val = v32->p;
+  return d;
+}
+
+void Solver::color_level(Level& L, int smoother) {
+  const int n = L.A.n;
+  const int g = grid_for(n, 256);
+  DBuf<int> color(n, s), newc(n, s), set, ctr(1, s);
+  color.fill_bytes(0xff);  // -1
+  bool cf_split = (smoother == SMOOTHER_CF_GS);
+  if (cf_split) {
+    set.alloc(n, s);
+    BN_LAUNCH(k_cf_set, g, 256, 0, s, L.cf.p, n, set.p);
+  }
+  int done = 0, round = 0;
+  while (done < n) {
+    BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
+    ctr.zero();
+    BN_LAUNCH(k_color_round, g, 256, 0, s, L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, n,
+              color.p, newc.p, ctr.p);
+    BN_LAUNCH(k_color_commit, g, 256, 0, s, n, newc.p, color.p);
+    done += read_scalar(ctr.p, s);
+    round++;
+  }
+  DBuf<int> key(n, s), ids(n, s), key_out(n, s);
+  L.gs_rows.alloc(n, s);
+  BN_LAUNCH(k_color_keys, g, 256, 0, s, cf_split ? set.p : nullptr, color.p, n, key.p, ids.p);
+  size_t tmp = 0;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n,
+                                          0, 7, s));
+  DBuf<unsigned char> t(tmp, s);
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n, 0, 7,
+                                          s));
+  std::vector<int> hk(n);
+  key_out.download(hk.data(), n);
+  BN_CUDA(cudaStreamSynchronize(s));
+  L.cptr.clear();
+  L.cjac.clear();
+  L.cptr.push_back(0);
+  for (int i = 1; i <= n; i++) {
+    if (i == n || hk[i] != hk[i - 1]) {
+      L.cptr.push_back(i);
+      L.cjac.push_back((hk[i - 1] & 63) == kMaxColors ? 1 : 0);
+    }
+  }
+  L.colored_for = smoother;
+  L.color_rounds = round;
+  const double avg = n > 0 ? (double)L.A.nnz / n : 0.0;
+  L.gs_group = avg <= 12.0 ? 1 : (avg <= 48.0 ? 8 : 32);
+}
+
+void Solver::alloc_vectors() {
+  const int nl = (int)lv.size();
+  for (int l = 0; l < nl; l++) {
+    Level& L = *lv[l];
+    int n = L.A.n;
+    if (l > 0) { L.b.alloc(n, s); L.x.alloc(n, s); }
+    if (l < nl - 1) L.r.alloc(n, s);
+    if (opt.precision == AMG_PREC_MIXED) {
+      if (l > 0) { L.b32.alloc(n, s); L.x32.alloc(n, s); }
+      if (l < nl - 1) L.r32.alloc(n, s);
+    }
+  }
+  const int n0 = n();
+  for (auto* v : {&u1, &r1, &icy, &icx, &xx, &r2, &corr}) v->alloc(n0, s);
+  for (auto* v : {&b, &x, &r, &z, &p, &ap}) v->alloc(n0, s);
+  if (opt.precision == AMG_PREC_MIXED)
+    for (auto* v : {&g32, &u1f, &r1f, &icyf, &icxf, &xxf, &r2f, &corrf}) v->alloc(n0, s);
+  sc.alloc(SC_COUNT, s);
+  sc.zero();
+  part0.alloc(kRedBlocks > spmv_grid(n0) ? kRedBlocks : spmv_grid(n0), s);
+  part1.alloc(kRedBlocks, s);
+  if (!h_sc) BN_CUDA(cudaMallocHost((void**)&h_sc, sizeof(double) * SC_COUNT));
+}
+
+void Solver::prepare_f32() {
+  const int nl = (int)lv.size();
+  for (int l = 0; l < nl; l++) {
+    Level& L = *lv[l];
+    L.A32.alloc(L.A.nnz > 0 ? L.A.nnz : 1, s);
+    BN_LAUNCH(k_to_f32<float>, grid_for(L.A.nnz, 256), 256, 0, s, L.A.val.p, (size_t)L.A.nnz,
+              L.A32.p);
+    if (l < nl - 1) {
+      L.P32.alloc(L.P.nnz > 0 ? L.P.nnz : 1, s);
+      L.R32.alloc(L.R.nnz > 0 ? L.R.nnz : 1, s);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.P.nnz, 256), 256, 0, s, L.P.val.p, (size_t)L.P.nnz,
+                L.P32.p);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.R.nnz, 256), 256, 0, s, L.R.val.p, (size_t)L.R.nnz,
+                L.R32.p);
+      if (L.l1.n) {
+        L.l1_32.alloc(L.l1.n, s);
+        BN_LAUNCH(k_to_f32<float>, grid_for(L.l1.n, 256), 256, 0, s, L.l1.p, L.l1.n, L.l1_32.p);
+      }
+      if (L.dg.n) {
+        L.dg32.alloc(L.dg.n, s);
+        BN_LAUNCH(k_to_f32<float>, grid_for(L.dg.n, 256), 256, 0, s, L.dg.p, L.dg.n, L.dg32.p);
+      }
+    }
+  }
+  if (own_solve) {
+    Aown32.alloc(Aown.nnz > 0 ? Aown.nnz : 1, s);
+    BN_LAUNCH(k_to_f32<float>, grid_for(Aown.nnz, 256), 256, 0, s, Aown.val.p, (size_t)Aown.nnz,
+              Aown32.p);
+  }
+  f32_ready = true;
+}
+
+void Solver::finish_setup() {
+  const int nl = (int)lv.size();
+  { Phase ph("dense coarse", s, nl - 1); coarse.setup(lv[nl - 1]->A, s); }
+  for (int l = 0; l < nl - 1; l++) {
+    Level& L = *lv[l];
+    const int sm = opt.smoother;
+    if ((sm == SMOOTHER_CF_GS || sm == SMOOTHER_GS) && L.colored_for != sm) {
+      Phase ph("colouring", s, l);
+      color_level(L, sm);
+    }
+    if (sm == SMOOTHER_L1 && L.l1.n == 0) {
+      L.l1.alloc(L.A.n, s);
+      BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.A.ia.p, L.A.val.p, L.A.n, L.l1.p);
+    }
+    if (sm == SMOOTHER_JACOBI && L.dg.n == 0) {
+      L.dg.alloc(L.A.n, s);
+      BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.A.ia.p, L.A.ja.p, L.A.val.p, L.A.n,
+                L.dg.p);
+    }
+  }
+  ic.want_f32 = (opt.precision == AMG_PREC_MIXED);
+  { Phase ph("ichol factor", s); ic.factor(Asolve(), s); }
+  f32_ready = false;
+  if (opt.precision == AMG_PREC_MIXED) { Phase ph("fp32 copies", s); prepare_f32(); }
+  { Phase ph("vectors", s); alloc_vectors(); }
+  drop_graphs();
+}
+
+// Hierarchy loop of amg_build_hierarchy (build_hierarchy.c:59-147).
+void Solver::build(CSR&& A0) {
+  cudaEventRecord(ev0, s);
+  lv.clear();
+  lv.emplace_back(new Level());
+  lv[0]->A = std::move(A0);
+  const int max_levels =
+      (opt.max_levels > 0 && opt.max_levels <= AMG_MAX_LEVELS) ? opt.max_levels : AMG_MAX_LEVELS;
+  while (lv.back()->A.n >= opt.min_size && (int)lv.size() < max_levels) {
+    Level& cur = *lv.back();
+    const int nf = cur.A.n;
+    const int li = (int)lv.size() - 1;
+    { Phase ph("strength", s, li); strength(cur.A, opt.threshold, cur.S, &cur.max_lam, s); }
+    cur.cf.alloc(nf, s);
+    int nc;
+    { Phase ph("coarsen", s, li); nc = coarsen(cur.S, opt.coarsening, cur.max_lam, cur.cf.p, s); }
+    cur.n_coarse = nc;
+    if (nc == 0 || nc >= nf) break;  // coarsening stalled (:78-83)
+    { Phase ph("interpolation", s, li); interpolation(cur.A, cur.S, cur.cf.p, nc, cur.P, s); }
+    { Phase ph("transpose P", s, li); transpose(cur.P, cur.R, s, true); }
+    CSR Ac, Acs;
+    { Phase ph("rap", s, li); rap(cur.R, cur.A, cur.P, Ac, s); }
+    { Phase ph("symmetrize Ac", s, li); symmetrize(Ac, Acs, s); }
+    lv.emplace_back(new Level());
+    lv.back()->A = std::move(Acs);
+  }
+  finish_setup();
+  cudaEventRecord(ev1, s);
+  BN_CUDA(cudaEventSynchronize(ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  stats.setup_seconds = ms * 1e-3;
+}
+
+// amg_rebuild_values (build_hierarchy.c:170-242): same S, C/F and P pattern,
+// new A; recompute P values, RAP and symmetrisation level by level.
+void Solver::rebuild_values(CSR&& A0) {
+  cudaEventRecord(ev0, s);
+  lv[0]->A = std::move(A0);
+  const int nl = (int)lv.size();
+  for (int k = 0; k < nl - 1; k++) {
+    Level& cur = *lv[k];
+    interpolation_values(cur.A, cur.S, cur.cf.p, cur.P, s);
+    transpose(cur.P, cur.R, s, true);
+    CSR Ac, Acs;
+    rap(cur.R, cur.A, cur.P, Ac, s);
+    symmetrize(Ac, Acs, s);
+    Level& nxt = *lv[k + 1];
+    nxt.A = std::move(Acs);
+    nxt.l1.release();
+    nxt.dg.release();
+  }
+  lv[0]->l1.release();
+  lv[0]->dg.release();
+  own_solve = false;
+  Aown = CSR();
+  finish_setup();
+  cudaEventRecord(ev1, s);
+  BN_CUDA(cudaEventSynchronize(ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  stats.setup_seconds = ms * 1e-3;
+}
+
+// ------------------------------------------------------------ V-cycle
+template <class T>
+void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
+  Level& L = *lv[l];
+  const bool f64 = sizeof(T) == 8;
+  DevMat<T> A = mat<T>(L.A, &L.A32);
+  const int n = L.A.n;
+  for (int sweep = 0; sweep < opt.nu; sweep++) {
+    switch (opt.smoother) {
+      case SMOOTHER_CF_GS:
+      case SMOOTHER_GS: {
+        const int nseg = (int)L.cptr.size() - 1;
+        T* tmp = f64 ? (T*)L.r.p : (T*)L.r32.p;
+        for (int q = 0; q < nseg; q++) {
+          int c = forward ? q : nseg - 1 - q;
+          const int* rows = L.gs_rows.p + L.cptr[c];
+          const int nr = L.cptr[c + 1] - L.cptr[c];
+          if (L.cjac[c])
+            jacobi_class<T>(A, rows, nr, bb, xl, tmp, L.gs_group, s);
+          else
+            gs_color<T>(A, rows, nr, bb, xl, L.gs_group, s);
+        }
+        break;
+      }
+      case SMOOTHER_JACOBI: {
+        T* rr = f64 ? (T*)L.r.p : (T*)L.r32.p;
+        const T* d = f64 ? (const T*)L.dg.p : (const T*)L.dg32.p;
+        spmv<T>(SPMV_RES, A, xl, bb, rr, s);
+        BN_LAUNCH(k_scaled_update<T>, grid_for(n, 256), 256, 0, s, xl, rr, d, (T)opt.omega, n);
+        break;
+      }
+      default: {  // SMOOTHER_L1
+        T* rr = f64 ? (T*)L.r.p : (T*)L.r32.p;
+        const T* d = f64 ? (const T*)L.l1.p : (const T*)L.l1_32.p;
+        spmv<T>(SPMV_RES, A, xl, bb, rr, s);
+        BN_LAUNCH(k_scaled_update<T>, grid_for(n, 256), 256, 0, s, xl, rr, d, (T)1, n);
+        break;
+      }
+    }
+  }
+}
+
+// backslash_rec (amg_cycle.c:180-212); xl is zero on entry
+template <class T>
+void Solver::backslash(int l, const T* bb, T* xl) {
+  const int nl = (int)lv.size();
+  if (l == nl - 1) {
+    coarse.apply<T>(bb, xl, s);
+    return;
+  }
+  Level& L = *lv[l];
+  Level& C = *lv[l + 1];
+  const bool f64 = sizeof(T) == 8;
+  T* rr = f64 ? (T*)L.r.p : (T*)L.r32.p;
+  T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
+  T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
+  { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
+  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.A, &L.A32), xl, bb, rr, s); }
+  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32), rr, nullptr, cb, s); }
+  if (l + 1 < nl - 1) vzero<T>(cx, C.A.n, s);
+  backslash<T>(l + 1, cb, cx);
+  spmv<T>(SPMV_ADD, mat<T>(L.P, &L.P32), cx, nullptr, xl, s);  // x += P ec
+}
+
+// fwdslash_rec (amg_cycle.c:222-253); xl is zero on entry, so the first
+// residual is b itself and the prolongation overwrites xl
+template <class T>
+void Solver::fwdslash(int l, const T* bb, T* xl) {
+  const int nl = (int)lv.size();
+  if (l == nl - 1) {
+    coarse.apply<T>(bb, xl, s);
+    return;
+  }
+  Level& L = *lv[l];
+  Level& C = *lv[l + 1];
+  const bool f64 = sizeof(T) == 8;
+  T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
+  T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
+  spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32), bb, nullptr, cb, s);  // rc = P^T b
+  fwdslash<T>(l + 1, cb, cx);
+  spmv<T>(SPMV_Y, mat<T>(L.P, &L.P32), cx, nullptr, xl, s);  // x = P ec
+  smooth<T>(l, bb, xl, false);
+}
+
+// amg_ichol_apply (amg_ichol_precond.c:22-48):
+//   u1 = backslash(g); x = u1 + IC^{-1}(g - A u1); x += fwdslash(g - A x)
+template <class T>
+void Solver::precond_t(const T* g, T* out) {
+  const bool f64 = sizeof(T) == 8;
+  const int n0 = n();
+  T* U1 = f64 ? (T*)u1.p : (T*)u1f.p;
+  T* R1 = f64 ? (T*)r1.p : (T*)r1f.p;
+  T* IY = f64 ? (T*)icy.p : (T*)icyf.p;
+  T* IX = f64 ? (T*)icx.p : (T*)icxf.p;
+  T* XX = f64 ? (T*)xx.p : (T*)xxf.p;
+  T* R2 = f64 ? (T*)r2.p : (T*)r2f.p;
+  T* CO = f64 ? (T*)corr.p : (T*)corrf.p;
+  DevMat<T> As = own_solve ? mat<T>(Aown, &Aown32) : mat<T>(lv[0]->A, &lv[0]->A32);
+  vzero<T>(U1, n0, s);
+  { Phase ph("backslash", s); backslash<T>(0, g, U1); }
+  { Phase ph("residual r1", s); spmv<T>(SPMV_RES, As, U1, g, R1, s); }
+  { Phase ph("ichol solve", s); ic.solve<T>(R1, IY, IX, s); }
+  vadd<T>(U1, IX, n0, XX, s);
+  { Phase ph("residual r2", s); spmv<T>(SPMV_RES, As, XX, g, R2, s); }
+  { Phase ph("fwdslash", s); fwdslash<T>(0, R2, CO); }
+  vadd<T>(XX, CO, n0, out, s);
+}
+
+// z = M r for the PCG: r -> z (captured once per precision as a CUDA graph)
+void Solver::precond(const double* g, double* out) {
+  const int mode = opt.precision == AMG_PREC_MIXED ? 1 : 0;
+  const bool use_graph = (g == r.p && out == z.p) && !trace_on();
+  if (use_graph && graph[mode]) {
+    BN_CUDA(cudaGraphLaunch(graph[mode], s));
+    g_launch_count += graph_kernels[mode];
+    return;
+  }
+  auto body = [&]() {
+    if (mode == 1) {
+      vconvert<float, double>(g, n(), g32.p, s);
+      precond_t<float>(g32.p, r2f.p);  // r2f is free once fwdslash has consumed it
+      vconvert<double, float>(r2f.p, n(), out, s);
+    } else {
+      precond_t<double>(g, out);
+    }
+  };
+  if (!use_graph) {
+    body();
+    return;
+  }
+  cudaGraph_t gr;
+  BN_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  unsigned long long before = g_launch_count;
+  try {
+    body();
+  } catch (...) {
+    cudaStreamEndCapture(s, &gr);
+    if (gr) cudaGraphDestroy(gr);
+    throw;
+  }
+  BN_CUDA(cudaStreamEndCapture(s, &gr));
+  graph_kernels[mode] = g_launch_count - before;  // kernels recorded, launched on replay
+  g_launch_count = before;
+  BN_CUDA(cudaGraphInstantiate(&graph[mode], gr, 0));
+  cudaGraphDestroy(gr);
+  BN_CUDA(cudaGraphLaunch(graph[mode], s));
+  g_launch_count += graph_kernels[mode];
+}
+
+// amg_pcg (amg_pcg.c:12-101) on device vectors.  FP64 throughout; the mixed
+// form uses the flexible (Polak-Ribiere) beta because its preconditioner is
+// not exactly symmetric.
+int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int print_level) {
+  const int n0 = n();
+  const bool flexible = (opt.precision == AMG_PREC_MIXED);
+  if (flexible && !f32_ready) prepare_f32();
+  DevMat<double> A = mat<double>(Asolve(), nullptr);
+  const int sg = spmv_grid(n0);
+  cudaEventRecord(ev0, s);
+  BN_CUDA(cudaMemcpyAsync(b.p, d_b, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  BN_CUDA(cudaMemcpyAsync(x.p, d_x, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  spmv<double>(SPMV_RES, A, x.p, b.p, r.p, s);            // r = b - A x
+  dot_partials<double>(b.p, b.p, r.p, n0, part0.p, part1.p, s);
+  reduce_partials(part0.p, kRedBlocks, sc.p + SC_BB, s);  // b.b
+  reduce_partials(part1.p, kRedBlocks, sc.p + SC_RR, s);  // scratch
+  precond(r.p, z.p);                                      // z = M r
+  BN_CUDA(cudaMemcpyAsync(p.p, z.p, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  dot_partials<double>(r.p, z.p, r.p, n0, part0.p, part1.p, s);
+  reduce_partials(part0.p, kRedBlocks, sc.p + SC_RZ, s);   // r.z
+  reduce_partials(part1.p, kRedBlocks, sc.p + SC_RR, s);   // r.r
+  BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
+  BN_CUDA(cudaStreamSynchronize(s));
+  int icerr = ic.take_error(s);
+  if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+  double bnorm = sqrt(h_sc[SC_BB]);
+  if (bnorm == 0.0) bnorm = 1.0;
+  const double rz0 = h_sc[SC_RZ];
+  double rnorm = sqrt(h_sc[SC_RR]);
+  double bn_rel = 1.0;
+  if (print_level >= 1) {
+    fprintf(stderr, "  %4s  %8s  %8s  %6s\n", "iter", "||r||_B", "rel", "rho");
+    fprintf(stderr, "  %4d  %8.2e  %8.2e\n", 0, sqrt(rz0), 1.0);
+  }
+  int iter;
+  int status = BN_OK;
+  for (iter = 1; iter <= maxiter; iter++) {
+    spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s, p.p, part0.p);  // Ap, p.Ap
+    reduce_partials(part0.p, sg, sc.p + SC_PAP, s);
+    pcg_update_xr(x.p, r.p, p.p, ap.p, n0, sc.p, part0.p, s);      // x, r, r.r
+    reduce_partials(part0.p, kRedBlocks, sc.p + SC_RR, s);
+    if (flexible) {  // r_{k+1}.z_k before z is overwritten
+      dot_partials<double>(r.p, z.p, nullptr, n0, part1.p, nullptr, s);
+      reduce_partials(part1.p, kRedBlocks, sc.p + SC_RZOLD_NEW, s);
+    }
+    precond(r.p, z.p);
+    dot_partials<double>(r.p, z.p, nullptr, n0, part0.p, nullptr, s);
+    reduce_partials(part0.p, kRedBlocks, sc.p + SC_RZNEW, s);
+    pcg_scalars(sc.p, flexible ? 1 : 0, s);
+    BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
+    BN_CUDA(cudaStreamSynchronize(s));
+    icerr = ic.take_error(s);
+    if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+    const double rz_new = h_sc[SC_RZ];  // rotated: SC_RZ now holds r_{k+1}.z_{k+1}
+    rnorm = sqrt(h_sc[SC_RR]);
+    bn_rel = sqrt(rz_new / rz0);
+    if (print_level >= 1)
+      fprintf(stderr, "  %4d  %8.2e  %8.2e  %6.4f\n", iter, sqrt(rz_new), bn_rel,
+              rz_new / h_sc[SC_RZ_PREV]);
+    if (!isfinite(rz_new) || !isfinite(rnorm)) {
+      status = BN_ERR_NAN;
+      iter = maxiter + 1;
+      break;
+    }
+    const double crit = (opt.stop == AMG_STOP_RELRES) ? rnorm / bnorm : bn_rel;
+    if (crit < tol) break;
+    pcg_update_p(p.p, z.p, n0, sc.p, s);
+  }
+  // true residual for the stats
+  spmv<double>(SPMV_RES, A, x.p, b.p, ap.p, s);
+  dot_partials<double>(ap.p, ap.p, nullptr, n0, part0.p, nullptr, s);
+  reduce_partials(part0.p, kRedBlocks, sc.p + SC_RR, s);
+  BN_CUDA(cudaMemcpyAsync(d_x, x.p, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  cudaEventRecord(ev1, s);
+  BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
+  BN_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  stats.solve_seconds = ms * 1e-3;
+  stats.relres = sqrt(h_sc[SC_RR]) / bnorm;
+  stats.bnorm_rel = bn_rel;
+  if (iter > maxiter) {
+    if (status == BN_OK) status = BN_ERR_NOT_CONVERGED;
+    fprintf(stderr, "  PCG: no convergence after %d iterations, relres = %.2e\n", maxiter,
+            rnorm / bnorm);
+    stats.iterations = maxiter;
+    stats.converged = 0;
+    set_last_error(status, status == BN_ERR_NAN ? "PCG: non-finite value in the iteration"
+                                                : "PCG: no convergence");
+    return -maxiter;
+  }
+  stats.iterations = iter;
+  stats.converged = 1;
+  set_last_error(BN_OK, "");
+  return iter;
+}
+
+// ------------------------------------------------------------ host helpers
+static thread_local int t_status = 0;
+static thread_local std::string t_msg;
+void set_last_error(int code, const std::string& msg) {
+  t_status = code;
+  t_msg = msg;
+}
+
+static int current_device_count() {
+  int c = 0;
+  if (cudaGetDeviceCount(&c) != cudaSuccess) return 0;
+  return c;
+}
+
+// Upload host CSR (validated), symmetrise on the device.
+static void upload_symmetrize(Solver& S, int n, int nnz, const int* ia, const int* ja,
+                              const double* val, bool device_ptrs, CSR& out) {
+  BN_REQUIRE(n > 0 && nnz >= 0 && ia && ja && val, BN_ERR_ARG, "invalid CSR arguments");
+  CSR Ain;
+  Ain.alloc(n, n, nnz, S.s, true);
+  auto kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  BN_CUDA(cudaMemcpyAsync(Ain.ia.p, ia, sizeof(int) * (n + 1), kind, S.s));
+  BN_CUDA(cudaMemcpyAsync(Ain.ja.p, ja, sizeof(int) * (size_t)nnz, kind, S.s));
+  BN_CUDA(cudaMemcpyAsync(Ain.val.p, val, sizeof(double) * (size_t)nnz, kind, S.s));
+  int f = validate(Ain.ia.p, Ain.ja.p, n, n, nnz, S.s);
+  BN_REQUIRE(!(f & 1), BN_ERR_ARG, "CSR row pointers are not a valid 0-based prefix array");
+  BN_REQUIRE(!(f & 2), BN_ERR_ARG, "CSR column index out of range");
+  BN_REQUIRE(!(f & 4), BN_ERR_DUP, "CSR row holds a duplicate column index");
+  symmetrize(Ain, out, S.s);
+}
+
+static Solver* make_solver(int n, int nnz, const int* ia, const int* ja, const double* val,
+                           const amg_b200_options* o, bool device_ptrs) {
+  BN_REQUIRE(current_device_count() > 0, BN_ERR_NO_DEVICE, "no CUDA device available");
+  std::unique_ptr<Solver> S(new Solver());
+  S->opt = *o;
+  if (S->opt.nu <= 0) S->opt.nu = 1;
+  if (S->opt.max_levels <= 0 || S->opt.max_levels > AMG_MAX_LEVELS)
+    S->opt.max_levels = AMG_MAX_LEVELS;
+  S->device = o->device;
+  BN_CUDA(cudaSetDevice(S->device));
+  BN_CUDA(cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking));
+  BN_CUDA(cudaEventCreate(&S->ev0));
+  BN_CUDA(cudaEventCreate(&S->ev1));
+  CSR A;
+  upload_symmetrize(*S, n, nnz, ia, ja, val, device_ptrs, A);
+  S->build(std::move(A));
+  return S.release();
+}
+
+template <class F>
+static int guarded(F&& f, int fail) {
+  try {
+    return f();
+  } catch (const Error& e) {
+    set_last_error(e.code, e.what());
+    return fail;
+  } catch (const std::exception& e) {
+    set_last_error(BN_ERR_CUDA, e.what());
+    return fail;
+  }
+}
+
+}  // namespace bn
+
+using bn::Solver;
+
+// ======================================================================
+//                               C ABI
+// ======================================================================
+BN_API void amg_b200_default_options(amg_b200_options* o) {
+  if (!o) return;
+  o->threshold = 0.25;
+  o->min_size = 500;
+  o->max_levels = AMG_MAX_LEVELS;
+  o->nu = 1;
+  o->coarsening = COARSEN_PMIS;
+  o->smoother = SMOOTHER_CF_GS;
+  o->omega = 0.5;
+  o->precision = AMG_PREC_FP64;
+  o->stop = AMG_STOP_BNORM;
+  o->device = 0;
+}
+
+BN_API void* amg_solver_create_ex(int n, int nnz, const int* ia, const int* ja,
+                                  const double* val, const amg_b200_options* opt) {
+  Solver* out = nullptr;
+  amg_b200_options o;
+  amg_b200_default_options(&o);
+  if (opt) o = *opt;
+  bn::guarded([&]() { out = bn::make_solver(n, nnz, ia, ja, val, &o, false); return 0; }, -1);
+  if (out) bn::set_last_error(0, "");
+  return out;
+}
+
+BN_API void* amg_solver_create_device(int n, int nnz, const int* ia, const int* ja,
+                                      const double* val, const amg_b200_options* opt) {
+  Solver* out = nullptr;
+  amg_b200_options o;
+  amg_b200_default_options(&o);
+  if (opt) o = *opt;
+  bn::guarded([&]() { out = bn::make_solver(n, nnz, ia, ja, val, &o, true); return 0; }, -1);
+  if (out) bn::set_last_error(0, "");
+  return out;
+}
+
+BN_API void* amg_solver_create(int n, int nnz, const int* ia, const int* ja, const double* val,
+                               double threshold, int min_size, int max_levels, int nu) {
+  amg_b200_options o;
+  amg_b200_default_options(&o);
+  o.threshold = threshold;
+  o.min_size = min_size;
+  o.max_levels = max_levels;
+  o.nu = nu;
+  return amg_solver_create_ex(n, nnz, ia, ja, val, &o);
+}
+
+BN_API int amg_solver_update(void* h, int n, int nnz, const int* ia, const int* ja,
+                             const double* val) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    BN_REQUIRE(n == S->lv[0]->A.n, bn::BN_ERR_ARG, "update: dimension differs from the hierarchy");
+    bn::CSR A;
+    bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
+    BN_REQUIRE(A.nnz == S->lv[0]->A.nnz, bn::BN_ERR_ARG, "update: sparsity differs");
+    S->rebuild_values(std::move(A));
+    bn::set_last_error(0, "");
+    return 0;
+  }, bn::BN_ERR_ARG);
+}
+
+BN_API int amg_solver_set_matrix(void* h, int n, int nnz, const int* ia, const int* ja,
+                                 const double* val) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    BN_REQUIRE(n == S->lv[0]->A.n, bn::BN_ERR_ARG, "set_matrix: dimension differs");
+    bn::CSR A;
+    bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
+    S->Aown = std::move(A);
+    S->own_solve = true;
+    S->ic.want_f32 = (S->opt.precision == AMG_PREC_MIXED);
+    S->ic.factor(S->Aown, S->s);
+    S->f32_ready = false;
+    if (S->opt.precision == AMG_PREC_MIXED) S->prepare_f32();
+    S->drop_graphs();
+    bn::set_last_error(0, "");
+    return 0;
+  }, bn::BN_ERR_ARG);
+}
+
+BN_API void amg_solver_set_smoother(void* h, int smoother, double omega) {
+  if (!h) return;
+  Solver* S = (Solver*)h;
+  bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    S->opt.smoother = smoother;
+    if (smoother == SMOOTHER_JACOBI) S->opt.omega = omega;
+    const int nl = (int)S->lv.size();
+    for (int l = 0; l < nl - 1; l++) {
+      bn::Level& L = *S->lv[l];
+      if ((smoother == SMOOTHER_CF_GS || smoother == SMOOTHER_GS) && L.colored_for != smoother)
+        S->color_level(L, smoother);
+      if (smoother == SMOOTHER_L1 && L.l1.n == 0) {
+        L.l1.alloc(L.A.n, S->s);
+        BN_LAUNCH(bn::k_l1_diag, bn::grid_for(L.A.n, 256), 256, 0, S->s, L.A.ia.p, L.A.val.p,
+                  L.A.n, L.l1.p);
+      }
+      if (smoother == SMOOTHER_JACOBI && L.dg.n == 0) {
+        L.dg.alloc(L.A.n, S->s);
+        BN_LAUNCH(bn::k_diag, bn::grid_for(L.A.n, 256), 256, 0, S->s, L.A.ia.p, L.A.ja.p,
+                  L.A.val.p, L.A.n, L.dg.p);
+      }
+    }
+    if (S->opt.precision == AMG_PREC_MIXED) S->prepare_f32();
+    S->drop_graphs();
+    return 0;
+  }, -1);
+}
+
+BN_API int amg_solver_set_precision(void* h, int precision) {
+  if (!h) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_REQUIRE(precision == AMG_PREC_FP64 || precision == AMG_PREC_MIXED, bn::BN_ERR_ARG,
+               "unknown precision");
+    BN_CUDA(cudaSetDevice(S->device));
+    S->opt.precision = precision;
+    if (precision == AMG_PREC_MIXED) {
+      if (!S->ic.fval32.n) {
+        S->ic.want_f32 = true;
+        S->ic.refresh_values();
+      }
+      S->prepare_f32();
+      S->alloc_vectors();
+    }
+    S->drop_graphs();
+    return 0;
+  }, bn::BN_ERR_ARG);
+}
+
+BN_API int amg_solver_set_stop(void* h, int stop) {
+  if (!h) return bn::BN_ERR_ARG;
+  ((Solver*)h)->opt.stop = stop;
+  return 0;
+}
+
+BN_API int amg_solver_solve_device(void* h, const double* d_b, double* d_x, double tol,
+                                   int maxiter, int print_level) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  int out = 0;
+  int rc = bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    out = S->pcg(d_b, d_x, tol, maxiter, print_level);
+    return 0;
+  }, -1);
+  return rc < 0 ? -maxiter : out;
+}
+
+BN_API int amg_solver_solve(void* h, const double* b, double* x, double tol, int maxiter,
+                            int print_level) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  int out = 0;
+  int rc = bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    const int n = S->n();
+    bn::DBuf<double> db(n, S->s), dx(n, S->s);
+    db.upload(b, n);
+    dx.upload(x, n);
+    out = S->pcg(db.p, dx.p, tol, maxiter, print_level);
+    dx.download(x, n);
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    return 0;
+  }, -1);
+  return rc < 0 ? -maxiter : out;
+}
+
+BN_API int amg_solver_precond(void* h, const double* g, double* xo) {
+  if (!h) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    const int n = S->n();
+    if (S->opt.precision == AMG_PREC_MIXED && !S->f32_ready) S->prepare_f32();
+    bn::DBuf<double> dg(n, S->s), dx(n, S->s);
+    dg.upload(g, n);
+    S->precond(dg.p, dx.p);
+    dx.download(xo, n);
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    int e = S->ic.take_error(S->s);
+    BN_REQUIRE(e == 0, e, "IC(0) solve: a bounded dependency wait ran out");
+    return 0;
+  }, bn::BN_ERR_CUDA);
+}
+
+BN_API int amg_solver_size(void* h) { return h ? ((Solver*)h)->n() : 0; }
+BN_API int amg_solver_num_levels(void* h) { return h ? (int)((Solver*)h)->lv.size() : 0; }
+
+BN_API void amg_solver_free(void* h) {
+  if (!h) return;
+  Solver* S = (Solver*)h;
+  cudaSetDevice(S->device);
+  cudaStream_t s = S->s;
+  delete S;
+  if (s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+}
+
+BN_API int amg_solver_stats(void* h, amg_solve_stats* out) {
+  if (!h || !out) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  S->stats.num_levels = (int)S->lv.size();
+  long long t = 0;
+  for (auto& L : S->lv) t += L->A.nnz;
+  S->stats.nnz_total = t;
+  S->stats.ichol_levels = S->ic.nlevels;
+  *out = S->stats;
+  return 0;
+}
+
+BN_API int amg_solver_level_info(void* h, int level, int* o) {
+  if (!h || !o) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  if (level < 0 || level >= (int)S->lv.size()) return bn::BN_ERR_ARG;
+  bn::Level& L = *S->lv[level];
+  const bool last = level == (int)S->lv.size() - 1;
+  o[0] = L.A.n;
+  o[1] = L.A.nnz;
+  o[2] = last ? 0 : L.S.nnz;
+  o[3] = last ? 0 : L.P.nnz;
+  o[4] = last ? 0 : L.n_coarse;
+  return 0;
+}
+
+BN_API int amg_solver_level_copy(void* h, int level, int* a_ia, int* a_ja, double* a_val,
+                                 int* s_ia, int* s_ja, double* s_val, int* p_ia, int* p_ja,
+                                 double* p_val, int* cf) {
+  if (!h) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  if (level < 0 || level >= (int)S->lv.size()) return bn::BN_ERR_ARG;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    bn::Level& L = *S->lv[level];
+    const bool last = level == (int)S->lv.size() - 1;
+    const int n = L.A.n;
+    if (a_ia) L.A.ia.download(a_ia, n + 1);
+    if (a_ja) L.A.ja.download(a_ja, L.A.nnz);
+    if (a_val) L.A.val.download(a_val, L.A.nnz);
+    if (!last) {
+      if (s_ia) L.S.ia.download(s_ia, n + 1);
+      if (s_ja) L.S.ja.download(s_ja, L.S.nnz);
+      if (s_val) L.S.val.download(s_val, L.S.nnz);
+      if (p_ia) L.P.ia.download(p_ia, n + 1);
+      if (p_ja) L.P.ja.download(p_ja, L.P.nnz);
+      if (p_val) L.P.val.download(p_val, L.P.nnz);
+      if (cf) L.cf.download(cf, n);
+    }
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    return 0;
+  }, bn::BN_ERR_CUDA);
+}
+
+BN_API const char* amg_solver_last_error(void) { return bn::t_msg.c_str(); }
+BN_API int amg_solver_last_status(void) { return bn::t_status; }
+BN_API unsigned long long amg_b200_launch_count(void) { return bn::g_launch_count; }

@@ -1,0 +1,206 @@
+/*
+ * amg_b200.h -- C ABI of the B200 AMG-PCG solver for vessel-network pressure
+ * systems.  Drop-in for the reference library (liuzhengqi1996/blood_network,
+ * C_amg1/lib/libamg.so): the same symbol names and signatures, host pointers
+ * in and out, computed on one NVIDIA B200 (sm_100a).  0-based CSR with int32
+ * indices and float64 values, exactly the reference's dcsr_mat.
+ *
+ * Link: -lamg_b200 (blood_network_b200/lib/libamg_b200.so).  No C++ or torch
+ * types cross this boundary.
+ */
+#ifndef AMG_B200_H
+#define AMG_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------
+ * Types, identical in layout to the reference (C_amg1/include/agg_lib.h:37-44
+ * and C_amg1/include/amg.h:333-342).
+ * --------------------------------------------------------------------- */
+typedef struct {
+  int row;     /* number of rows */
+  int col;     /* number of columns */
+  int nnz;     /* number of nonzero entries */
+  int* ia;     /* row pointers, size row+1 */
+  int* ja;     /* column indices, size nnz */
+  double* val; /* values, size nnz */
+} dcsr_mat;
+
+#define AMG_MAX_LEVELS 20
+#define SMOOTHER_L1 0     /* l1-Jacobi */
+#define SMOOTHER_GS 1     /* Gauss-Seidel (multicolour on the device) */
+#define SMOOTHER_CF_GS 2  /* CF-ordered Gauss-Seidel (multicolour, C then F) */
+#define SMOOTHER_JACOBI 3 /* damped Jacobi */
+#define COARSEN_RS 0
+#define COARSEN_PMIS 1
+#define COARSEN_HMIS 2
+
+/* Status codes returned by the extension entry points and reported by
+ * amg_solver_last_status(). */
+#define AMG_OK 0
+#define AMG_ERR_ARG (-1)
+#define AMG_ERR_CUDA (-2)
+#define AMG_ERR_OOM (-3)
+#define AMG_ERR_NOT_CONVERGED (-4)
+#define AMG_ERR_NAN (-5)
+#define AMG_ERR_SPIN (-6)
+#define AMG_ERR_COARSE (-7)
+#define AMG_ERR_NO_DEVICE (-8)
+#define AMG_ERR_DUP (-9)
+
+/* Precision forms */
+#define AMG_PREC_FP64 0  /* everything FP64, standard PCG (the reference's) */
+#define AMG_PREC_MIXED 1 /* FP32 hierarchy + V-cycle inside FP64 flexible PCG */
+
+/* Stopping rules for the PCG */
+#define AMG_STOP_BNORM 0  /* sqrt(r.z / r0.z0) < tol  (the reference's rule) */
+#define AMG_STOP_RELRES 1 /* ||r||_2 / ||b||_2 < tol  (true relative residual) */
+
+/* =====================================================================
+ * Drop-in entry points (C_amg1/src/amg_wrapper.c)
+ * ===================================================================== */
+
+/* Replaces amg_solver_create (amg_wrapper.c:51-97).  Copies the host CSR to
+ * the device, symmetrises A=(A+A^T)/2, builds the AMG hierarchy (PMIS, CF
+ * Gauss-Seidel) and the fine-level IC(0).  max_levels outside 1..20 becomes
+ * 20; nu <= 0 becomes 1.  Returns NULL on failure (reason in
+ * amg_solver_last_error()). */
+void* amg_solver_create(int n, int nnz, const int* ia, const int* ja, const double* val,
+                        double threshold, int min_size, int max_levels, int nu);
+
+/* Replaces amg_solver_update (amg_wrapper.c:114-149): same sparsity, new
+ * values; recomputes P values, coarse operators and IC(0).  Returns 0. */
+int amg_solver_update(void* handle, int n, int nnz, const int* ia, const int* ja,
+                      const double* val);
+
+/* Replaces amg_solver_set_matrix (amg_wrapper.c:168-199): new solve matrix
+ * and fine IC(0); the hierarchy is kept.  Returns 0. */
+int amg_solver_set_matrix(void* handle, int n, int nnz, const int* ia, const int* ja,
+                          const double* val);
+
+/* Replaces amg_solver_set_smoother (amg_wrapper.c:241-246). */
+void amg_solver_set_smoother(void* handle, int smoother, double omega);
+
+/* Replaces amg_solver_solve (amg_wrapper.c:214-225).  Host b and x; x is the
+ * initial guess.  Returns the iteration count, or -maxiter when not
+ * converged.  print_level >= 1 prints per-iteration rows to stderr. */
+int amg_solver_solve(void* handle, const double* b, double* x, double tol, int maxiter,
+                     int print_level);
+
+/* Replace amg_solver_size / num_levels / free (amg_wrapper.c:249-268). */
+int amg_solver_size(void* handle);
+int amg_solver_num_levels(void* handle);
+void amg_solver_free(void* handle);
+
+/* =====================================================================
+ * Extensions (no counterpart in the reference's wrapper)
+ * ===================================================================== */
+typedef struct {
+  double threshold; /* strength threshold theta */
+  int min_size;     /* coarsening stops below this size */
+  int max_levels;   /* 1..20 */
+  int nu;           /* smoothing sweeps */
+  int coarsening;   /* COARSEN_RS / COARSEN_PMIS / COARSEN_HMIS (the reference
+                       selects this only in its CLI, test_amg.c:91) */
+  int smoother;     /* SMOOTHER_* */
+  double omega;     /* damped-Jacobi factor */
+  int precision;    /* AMG_PREC_FP64 / AMG_PREC_MIXED */
+  int stop;         /* AMG_STOP_BNORM / AMG_STOP_RELRES */
+  int device;       /* CUDA device ordinal */
+} amg_b200_options;
+
+/* Defaults: theta 0.25, min_size 500, 20 levels, nu 1, PMIS, CF-GS, omega
+ * 0.5, FP64, B-norm stop, device 0. */
+void amg_b200_default_options(amg_b200_options* opt);
+
+/* Create with explicit options (host CSR). */
+void* amg_solver_create_ex(int n, int nnz, const int* ia, const int* ja, const double* val,
+                           const amg_b200_options* opt);
+/* Create from CSR already resident on the device (device pointers). */
+void* amg_solver_create_device(int n, int nnz, const int* d_ia, const int* d_ja,
+                               const double* d_val, const amg_b200_options* opt);
+
+int amg_solver_set_precision(void* handle, int precision);
+int amg_solver_set_stop(void* handle, int stop);
+
+/* Solve with device-resident b and x (x: initial guess in, solution out). */
+int amg_solver_solve_device(void* handle, const double* d_b, double* d_x, double tol,
+                            int maxiter, int print_level);
+
+/* One application of the AMG+IC(0) preconditioner, x = M g (host arrays),
+ * the reference's amg_ichol_precond (C_amg1/src/amg_ichol_precond.c:51). */
+int amg_solver_precond(void* handle, const double* g, double* x);
+
+typedef struct {
+  int iterations;       /* last solve */
+  int converged;
+  double relres;        /* true ||b - A x|| / ||b|| after the last solve */
+  double bnorm_rel;     /* sqrt(r.z / r0.z0) at exit */
+  double setup_seconds; /* device time of the last hierarchy build */
+  double solve_seconds; /* device time of the last solve */
+  int num_levels;
+  long long nnz_total;  /* sum of nnz over levels (operator complexity numerator) */
+  int ichol_levels;     /* dependency levels of the fine IC(0) */
+} amg_solve_stats;
+
+int amg_solver_stats(void* handle, amg_solve_stats* out);
+
+/* Per-level sizes: n, nnz(A), nnz(S), nnz(P), n_coarse. */
+int amg_solver_level_info(void* handle, int level, int* out5);
+/* Copy level data to host (any pointer may be NULL). */
+int amg_solver_level_copy(void* handle, int level, int* a_ia, int* a_ja, double* a_val,
+                          int* s_ia, int* s_ja, double* s_val, int* p_ia, int* p_ja,
+                          double* p_val, int* cf);
+
+const char* amg_solver_last_error(void);
+int amg_solver_last_status(void);
+unsigned long long amg_b200_launch_count(void);
+
+/* =====================================================================
+ * Kernel-level drop-ins: the reference's internal C entry points with host
+ * dcsr_mat in/out, computed on the device.  Outputs are malloc'd as the
+ * reference does (free with free()).
+ * ===================================================================== */
+
+/* rs_strength (C_amg1/src/rs_classical.c:30-88) */
+void rs_strength(const dcsr_mat* A, double theta, dcsr_mat* S, int* max_lam);
+/* pmis_coarsening (rs_classical.c:246-371); cf: +1 C, -1 F */
+void pmis_coarsening(const dcsr_mat* S, int* cf, int* n_coarse);
+/* hmis_coarsening (rs_classical.c:390-611): parallel RS first pass on the device */
+void hmis_coarsening(const dcsr_mat* S, int* cf, int* n_coarse);
+/* rs_coarsening (rs_classical.c:108-229): parallel RS first pass on the device */
+void rs_coarsening(const dcsr_mat* S, int max_lam, int* cf, int* n_coarse);
+/* rs_standard_interpolation[_sparsity|_values] (rs_classical.c:643-819) */
+void rs_standard_interpolation_sparsity(const dcsr_mat* S, const int* cf, dcsr_mat* P);
+void rs_standard_interpolation_values(const dcsr_mat* A, const dcsr_mat* S, const int* cf,
+                                      dcsr_mat* P);
+void rs_standard_interpolation(const dcsr_mat* A, const dcsr_mat* S, const int* cf,
+                               dcsr_mat* P);
+/* dcsr_rap (C_amg1/src/sparse_ops.c:102-213): rap_out = R A P */
+void dcsr_rap(dcsr_mat* r_in, dcsr_mat* a_in, dcsr_mat* p_in, dcsr_mat* rap_out);
+/* SpMV family (sparse_ops.c:19-75) */
+void abyvg(const int* ia, const int* ja, const double* a, const double* x, int n, double* y);
+void abyvcs(const int* ia, const int* ja, const double* a, const double* x, int n, double* y);
+void abyvam(const double* x, const int* ia, const int* ja, const double* a, const double* y,
+            int n, double* z);
+void vbya(const int* ia, const int* ja, const double* a, const double* x, int n, int m_dim,
+          double* y);
+
+/* IC(0) factor (C_amg1/include/amg.h:344-351, ichol.c:12-172) */
+typedef struct {
+  int n;
+  int* ia;
+  int* ja;
+  double* val;
+  int nnz;
+} ichol_factor;
+void ichol_compute(const dcsr_mat* A, ichol_factor* L);
+void ichol_solve(const ichol_factor* L, const double* b, double* x);
+void ichol_free(ichol_factor* L);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMG_B200_H */
