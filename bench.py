@@ -1,0 +1,386 @@
+#!/usr/bin/env python3
+"""Benchmark: time to relative residual 1e-8 on the 20M-node vascular network,
+mixed-precision vs FP64 AMG-PCG on one B200, plus fine-level SpMV HBM GB/s.
+
+One step = one PCG solve (AMG + IC(0) preconditioner) of the 20M-node
+network from x0 = 0 to a true relative residual <= 1e-8, with the matrix,
+the hierarchy and the right-hand side resident in HBM.  The headline `value`
+is the mixed-precision form (FP32 hierarchy and V-cycle inside FP64 flexible
+PCG); the plain FP64 form is timed the same way beside it.  `e2e` is the
+same metric through the C ABI with host buffers: amg_solver_create_ex from
+host CSR (setup included) + amg_solver_solve with host b/x.
+
+Run: python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Multi-GPU runs are replicas (one independent network solve per GPU): the
+single-network solve does not shard.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "time to rtol 1e-8, 20M-node net: mixed vs FP64 AMG-PCG, 1 B200; SpMV HBM GB/s"
+WORKLOAD = "vascular_20m"
+SAMPLE_DEPTH, SAMPLE_NODES = 18, 1_000_000   # bounded CPU sample, same generator/options
+
+
+def peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws <= 1:
+        return 0, 1, 0
+    import datetime
+    import torch.distributed as dist
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    import torch
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+    return rank, ws, local
+
+
+def max_over_ranks(v, ws):
+    if ws <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------- reference arm
+def reference_sample(steps, warmup, quiet=False):
+    """Time the reference C solver (compiled from its sources) on a bounded
+    sample of the workload: the same generator and options at 1M nodes."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import ref as R
+    from blood_network_b200.network import vascular_network, CONFIGS
+    cfg = CONFIGS[WORKLOAD]
+    net = vascular_network(SAMPLE_DEPTH, SAMPLE_NODES, seed=0,
+                           diffusive_fraction=cfg["diffusive_fraction"], keep_segments=False)
+    import scipy.sparse as sp
+    A = sp.csr_matrix((net.data, net.indices, net.indptr), shape=(net.n, net.n))
+    # loosest B-norm tolerance (the reference's stopping rule) that reaches a
+    # true relative residual <= 1e-8
+    tol_used = None
+    for tol in (1e-6, 1e-7, 1e-8, 1e-9, 1e-10):
+        it, ts, tv, x = R.ref_timed(net.n, net.indptr, net.indices, net.data, net.rhs,
+                                    cfg["theta"], 500, 1, 2, tol, 500)
+        rr = np.linalg.norm(net.rhs - A @ x) / np.linalg.norm(net.rhs)
+        if rr <= 1e-8:
+            tol_used = tol
+            break
+    times = []
+    for k in range(warmup + steps):
+        it, ts, tv, x = R.ref_timed(net.n, net.indptr, net.indices, net.data, net.rhs,
+                                    cfg["theta"], 500, 1, 2, tol_used, 500)
+        if k >= warmup:
+            times.append((ts, tv, it))
+    rr = float(np.linalg.norm(net.rhs - A @ x) / np.linalg.norm(net.rhs))
+    return net, times, tol_used, rr
+
+
+def _sample_job(steps, warmup):
+    net, times, tol_used, rr = reference_sample(steps, warmup)
+    return net.n, net.nnz, times, tol_used, rr
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from blood_network_b200.network import CONFIGS
+    nnz_target = 103_215_590  # nnz of the 20M-node workload (seed 0)
+    net, times, tol_used, rr = reference_sample(args.steps, args.warmup)
+    scale = nnz_target / net.nnz
+    solve = statistics.mean(t[1] for t in times) * scale
+    total = statistics.mean(t[0] + t[1] for t in times) * scale
+    sample = (f"reference C solver (C_amg1, -O3, 1 thread) on the same generator and options "
+              f"at n={net.n}, nnz={net.nnz} (HMIS theta 0.5, diffusive 30%), B-norm tol "
+              f"{tol_used:g} -> true relres {rr:.1e}; times scaled by nnz ratio {scale:.2f}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": solve, "unit": "s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": solve * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "precision": "fp64 (reference)",
+                   "iterations": times[-1][2], "setup_s_scaled":
+                   statistics.mean(t[0] for t in times) * scale},
+        "cpu_baseline": {"value": solve, "unit": "s", "cores": 1, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": total, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- B200 arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(args.warmup, 3)
+
+    rank, ws, local = dist_init(args)
+    import torch
+    torch.cuda.set_device(local)
+    from blood_network_b200 import amg
+    from blood_network_b200.network import make_config, CONFIGS
+    cfg = CONFIGS[args.config]
+    coarsen = {"pmis": amg.COARSEN_PMIS, "hmis": amg.COARSEN_HMIS, "rs": amg.COARSEN_RS}[
+        cfg["coarsening"]]
+    net = make_config(args.config, keep_segments=False)
+    n, nnz = net.n, net.nnz
+    lib = amg.load_library()
+
+    # inputs resident in HBM
+    d_ia = torch.from_numpy(net.indptr).cuda()
+    d_ja = torch.from_numpy(net.indices).cuda()
+    d_val = torch.from_numpy(net.data).cuda()
+    d_b = torch.from_numpy(net.rhs).cuda()
+    d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    import ctypes as C
+    opt = amg.default_options(threshold=cfg["theta"], min_size=500, max_levels=20, nu=1,
+                              coarsening=coarsen, precision=amg.PREC_FP64,
+                              stop=amg.STOP_RELRES, device=local)
+    torch.cuda.synchronize()
+    h = lib.amg_solver_create_device(n, nnz, C.c_void_p(d_ia.data_ptr()),
+                                     C.c_void_p(d_ja.data_ptr()), C.c_void_p(d_val.data_ptr()),
+                                     C.byref(opt))
+    if not h:
+        raise RuntimeError(lib.amg_solver_last_error().decode())
+    st = amg.Stats()
+    lib.amg_solver_stats(h, C.byref(st))
+    setup_s = st.setup_seconds
+    levels = st.num_levels
+    op_cx = st.nnz_total / nnz
+
+    def solve_steps(prec, k, w):
+        lib.amg_solver_set_precision(h, prec)
+        dev, its, rel = [], [], []
+        for i in range(w + k):
+            d_x.zero_()
+            torch.cuda.synchronize()
+            if i == w:
+                barrier(ws)
+                torch.cuda.synchronize()
+                launches0 = lib.amg_b200_launch_count()
+            it = lib.amg_solver_solve_device(h, C.c_void_p(d_b.data_ptr()),
+                                             C.c_void_p(d_x.data_ptr()), 1e-8, 200, 0)
+            lib.amg_solver_stats(h, C.byref(st))
+            if i >= w:
+                dev.append(st.solve_seconds)
+                its.append(it)
+                rel.append(st.relres)
+        torch.cuda.synchronize()
+        barrier(ws)
+        launches = lib.amg_b200_launch_count() - launches0
+        return dev, its, rel, launches
+
+    clocks = ClockSampler(local)
+    # FP64 form (beside), then the mixed form (headline) with clocks sampled
+    fp64_dev, fp64_its, fp64_rel, _ = solve_steps(amg.PREC_FP64, args.steps, args.warmup)
+    clocks.start()
+    mx_dev, mx_its, mx_rel, launches = solve_steps(amg.PREC_MIXED, args.steps, args.warmup)
+    clk = clocks.stop()
+
+    mixed_s = max_over_ranks(statistics.mean(mx_dev), ws)
+    fp64_s = max_over_ranks(statistics.mean(fp64_dev), ws)
+
+    # dominant-kernel roofline: fine-level residual SpMV r = b - A x
+    reps = 50
+    ms64 = C.c_double()
+    ms32 = C.c_double()
+    msgs = C.c_double()
+    lib.amg_solver_bench_kernel(h, 0, 0, reps, C.byref(ms64))
+    lib.amg_solver_bench_kernel(h, 0, 1, reps, C.byref(ms32))
+    lib.amg_solver_bench_kernel(h, 1, 1, reps, C.byref(msgs))
+    bytes64 = 12 * nnz + 4 * (n + 1) + 8 * n * 3      # val+ja, ia, x, b, r
+    bytes32 = 8 * nnz + 4 * (n + 1) + 4 * n * 3
+    bytes_gs32 = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n + 8 * n  # + row list, b, x r/w
+    peak, peak_kind = peaks()
+    gbs64 = bytes64 / (ms64.value * 1e-3) / 1e9
+    gbs32 = bytes32 / (ms32.value * 1e-3) / 1e9
+    gbs_gs = bytes_gs32 / (msgs.value * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(HERE, "profiles", "spmv_fp64_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI with host buffers (setup included)
+    e2e_k = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    e2e_times = []
+    hb = np.ascontiguousarray(net.rhs)
+    hx = np.zeros(n)
+    o2 = amg.default_options(threshold=cfg["theta"], min_size=500, max_levels=20, nu=1,
+                             coarsening=coarsen, precision=amg.PREC_MIXED,
+                             stop=amg.STOP_RELRES, device=local)
+    for i in range(1 + e2e_k):
+        hx[:] = 0.0
+        torch.cuda.synchronize()
+        barrier(ws)
+        t0 = time.perf_counter()
+        h2 = lib.amg_solver_create_ex(n, nnz, amg._p(net.indptr), amg._p(net.indices),
+                                      amg._p(net.data), C.byref(o2))
+        it2 = lib.amg_solver_solve(h2, amg._p(hb), amg._p(hx), 1e-8, 200, 0)
+        t1 = time.perf_counter()
+        lib.amg_solver_free(h2)
+        if i >= 1:
+            e2e_times.append(t1 - t0)
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), ws)
+    import scipy.sparse as sp
+    A_host = sp.csr_matrix((net.data, net.indices, net.indptr), shape=(n, n))
+    e2e_rel = float(np.linalg.norm(net.rhs - A_host @ hx) / np.linalg.norm(net.rhs))
+    h2d = 4 * (n + 1) + 4 * nnz + 8 * nnz + 8 * n + 8 * n
+    d2h = 8 * n
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            import multiprocessing as mp
+            with mp.get_context("spawn").Pool(1) as pool:  # no CUDA in the child
+                snet_n, snet_nnz, times, tol_used, rr = pool.apply(_sample_job, (1, 0))
+
+            class _S:
+                n, nnz = snet_n, snet_nnz
+            snet = _S
+            scale = nnz / snet.nnz
+            cpu = {"value": statistics.mean(t[1] for t in times) * scale, "unit": "s", "cores": 1,
+                   "kind": "reference",
+                   "sample": (f"reference C solver (1 thread) on the same generator/options at "
+                              f"n={snet.n}, nnz={snet.nnz}, B-norm tol {tol_used:g} (true relres "
+                              f"{rr:.1e}); solve time scaled by nnz ratio {scale:.2f}; setup "
+                              f"{statistics.mean(t[0] for t in times) * scale:.1f} s scaled")}
+        except Exception as e:  # the checker library is optional at run time
+            cpu = {"value": None, "unit": "s", "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    lib.amg_solver_free(h)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": mixed_s, "unit": "s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed_s * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 V-cycle + f64 PCG", "data": "synthetic",
+            "config": {"workload": f"{args.config}: n={n}, nnz={nnz}, HMIS theta "
+                                   f"{cfg['theta']}, direct interpolation, CF-GS nu=1, "
+                                   f"coarsest<=500 dense FP64, AMG+IC(0) preconditioner",
+                       "precision": "mixed (FP32 hierarchy/V-cycle in FP64 flexible PCG)",
+                       "stop": "true relative residual <= 1e-8, x0 = 0",
+                       "l2": "no flush: the resident system (>1.3 GB) exceeds the 126 MB L2",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "levels": levels, "operator_complexity": round(op_cx, 3),
+                       "setup_s": setup_s},
+            "fp64_solve_s": fp64_s,
+            "mixed_speedup_vs_fp64": fp64_s / mixed_s,
+            "iterations": {"mixed": mx_its[-1], "fp64": fp64_its[-1]},
+            "relres": {"mixed": max(mx_rel), "fp64": max(fp64_rel)},
+            "spmv": {"fp64_gbs": gbs64, "fp32_gbs": gbs32, "gs_sweep_fp32_gbs": gbs_gs,
+                     "fp64_ms": ms64.value, "fp32_ms": ms32.value},
+            "roofline": {"bound": "hbm", "achieved": gbs64, "peak": peak, "unit": "GB/s",
+                         "frac": gbs64 / peak, "traffic": traffic,
+                         "kernel": "fine-level residual SpMV r=b-Ax, FP64 CSR",
+                         "algorithmic_bytes": bytes64, "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "relres": e2e_rel},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -91,6 +91,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "amg_solver_stats": (i, [vp, C.POINTER(Stats)]),
         "amg_solver_level_info": (i, [vp, i, ip]),
         "amg_solver_level_copy": (i, [vp, i] + [vp] * 10),
+        "amg_solver_bench_kernel": (i, [vp, i, i, i, C.POINTER(C.c_double)]),
         "amg_solver_last_error": (C.c_char_p, []),
         "amg_solver_last_status": (i, []),
         "amg_b200_launch_count": (C.c_ulonglong, []),
@@ -224,6 +225,22 @@ class AMGSolver:
                                             _p(a.indices), _p(a.data))
         if rc != 0:
             raise AMGError(rc, self.lib.amg_solver_last_error().decode())
+
+    def bench_kernel(self, which, precision=0, reps=20):
+        ms = C.c_double()
+        rc = self.lib.amg_solver_bench_kernel(self.h, which, precision, reps, C.byref(ms))
+        if rc != 0:
+            raise AMGError(rc, self.lib.amg_solver_last_error().decode())
+        return ms.value
+
+    def solve_device(self, d_b, d_x, tol=1e-8, maxiter=200, print_level=0):
+        """Solve with device pointers (ints), e.g. torch tensors' data_ptr()."""
+        it = self.lib.amg_solver_solve_device(self.h, C.c_void_p(d_b), C.c_void_p(d_x), tol,
+                                              maxiter, print_level)
+        st = self.lib.amg_solver_last_status()
+        if st not in (0, -4, -5):
+            raise AMGError(st, self.lib.amg_solver_last_error().decode())
+        return it
 
     @property
     def num_levels(self):

@@ -169,6 +169,8 @@ static void spmv_api(int mode, const int* ia, const int* ja, const double* a, co
     if (mode == SPMV_RES) { db.alloc(n, s); db.upload(b, n); }
     DevMat<double> A;
     A.n = n; A.m = m; A.nnz = nnz; A.ia = dia.p; A.ja = dja.p; A.val = da.p;
+    // group 0 without long rows: every row summed by one thread in storage
+    // order, the reference's sequential order
     spmv<double>(mode, A, dx.p, db.p, dy.p, s);
     dy.download(y, n);
     BN_CUDA(cudaStreamSynchronize(s));

@@ -333,55 +333,121 @@ __global__ void k_rap_fill_huge(const int* __restrict__ ria, const int* __restri
 // appearance, which places the diagonal first.
 constexpr long long kSortProducts = 16384;
 
-__global__ void k_rap_gen_stream(const int* __restrict__ ria, const int* __restrict__ rja,
-                                 const double* __restrict__ rval, const int* __restrict__ aia,
-                                 const int* __restrict__ aja, const double* __restrict__ aval,
-                                 const int* __restrict__ pia, const int* __restrict__ pja,
-                                 const double* __restrict__ pval, const int* __restrict__ rows,
-                                 int m, const long long* __restrict__ poff,
+// products per (hub row, R entry) pair: sum over A row i1 of |P_i2|
+__global__ void k_pair_counts(const int* __restrict__ ria, const int* __restrict__ rja,
+                              const int* __restrict__ aia, const int* __restrict__ aja,
+                              const int* __restrict__ pia, const int* __restrict__ pair_row,
+                              const int* __restrict__ pair_k1, long long npairs,
+                              long long* __restrict__ cnt) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < npairs;
+       p += warps) {
+    const int k1 = pair_k1[p];
+    if (k1 < 0) {  // diagonal seed slot
+      if (lane == 0) cnt[p] = 1;
+      continue;
+    }
+    const int i1 = rja[k1];
+    long long c = 0;
+    for (int k2 = aia[i1] + lane; k2 < aia[i1 + 1]; k2 += 32) {
+      const int i2 = aja[k2];
+      c += pia[i2 + 1] - pia[i2];
+    }
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+    if (lane == 0) cnt[p] = c;
+  }
+}
+
+// list the (row, k1) pairs of the hub rows: row q owns pairs
+// [pstart[q], pstart[q+1]) and one extra leading slot for its diagonal seed
+__global__ void k_pairs(const int* __restrict__ ria, const int* __restrict__ rows, int m,
+                        const long long* __restrict__ pstart, int* __restrict__ pair_row,
+                        int* __restrict__ pair_k1) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+    const int ic = rows[q];
+    long long p = pstart[q];
+    pair_row[p] = q;   // seed slot
+    pair_k1[p] = -1;
+    p++;
+    for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++, p++) {
+      pair_row[p] = q;
+      pair_k1[p] = k1;
+    }
+  }
+}
+
+// warp per pair: write the pair's products at its stream offset, in order
+__global__ void k_rap_gen_stream(const int* __restrict__ rja, const double* __restrict__ rval,
+                                 const int* __restrict__ aia, const int* __restrict__ aja,
+                                 const double* __restrict__ aval, const int* __restrict__ pia,
+                                 const int* __restrict__ pja, const double* __restrict__ pval,
+                                 const int* __restrict__ rows, const int* __restrict__ pair_row,
+                                 const int* __restrict__ pair_k1, long long npairs,
+                                 const long long* __restrict__ poff,
                                  unsigned long long* __restrict__ keys,
                                  long long* __restrict__ idx, double* __restrict__ vals) {
   const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += warps) {
-    const int ic = rows[q];
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long pr = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; pr < npairs;
+       pr += warps) {
+    const int q = pair_row[pr];
     const unsigned long long hi = (unsigned long long)q << 32;
-    long long pos = poff[q];
-    if (lane == 0) {
-      keys[pos] = hi | (unsigned)ic;
-      idx[pos] = pos;
-      vals[pos] = 0.0;
-    }
-    pos++;
-    for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
-      const double r = rval[k1];
-      const int i1 = rja[k1];
-      const int a1 = aia[i1 + 1];
-      for (int base = aia[i1]; base < a1; base += 32) {
-        const int k2 = base + lane;
-        double ra = 0.0;
-        int p0 = 0, plen = 0;
-        if (k2 < a1) {
-          ra = xmul(r, aval[k2]);
-          const int i2 = aja[k2];
-          p0 = pia[i2];
-          plen = pia[i2 + 1] - p0;
-        }
-        int incl = plen;
-        for (int off = 1; off < 32; off <<= 1) {
-          int v = __shfl_up_sync(0xffffffffu, incl, off);
-          if (lane >= off) incl += v;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        const long long o = pos + incl - plen;
-        for (int q3 = 0; q3 < plen; q3++) {
-          keys[o + q3] = hi | (unsigned)pja[p0 + q3];
-          idx[o + q3] = o + q3;
-          vals[o + q3] = xmul(ra, pval[p0 + q3]);
-        }
-        pos += total;
+    long long pos = poff[pr];
+    const int k1 = pair_k1[pr];
+    if (k1 < 0) {  // diagonal seed: value 0.0 ahead of every product
+      if (lane == 0) {
+        keys[pos] = hi | (unsigned)rows[q];
+        idx[pos] = pos;
+        vals[pos] = 0.0;
       }
+      continue;
     }
+    const double r = rval[k1];
+    const int i1 = rja[k1];
+    const int a1 = aia[i1 + 1];
+    for (int base = aia[i1]; base < a1; base += 32) {
+      const int k2 = base + lane;
+      double ra = 0.0;
+      int p0 = 0, plen = 0;
+      if (k2 < a1) {
+        ra = xmul(r, aval[k2]);
+        const int i2 = aja[k2];
+        p0 = pia[i2];
+        plen = pia[i2 + 1] - p0;
+      }
+      int incl = plen;
+      for (int off = 1; off < 32; off <<= 1) {
+        int v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const long long o = pos + incl - plen;
+      for (int q3 = 0; q3 < plen; q3++) {
+        keys[o + q3] = hi | (unsigned)pja[p0 + q3];
+        idx[o + q3] = o + q3;
+        vals[o + q3] = xmul(ra, pval[p0 + q3]);
+      }
+      pos += total;
+    }
+  }
+}
+
+__global__ void k_seed_counts(long long* __restrict__ cnt, const int* __restrict__ pair_k1,
+                              long long npairs) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npairs;
+       p += (long long)gridDim.x * blockDim.x)
+    if (pair_k1[p] < 0) cnt[p] = 1;
+}
+
+// per hub row: number of column segments (= distinct columns)
+__global__ void k_seg_row_counts(const unsigned long long* __restrict__ keys,
+                                 const long long* __restrict__ seg, long long nseg,
+                                 const int* __restrict__ rows, int* __restrict__ cnt_out) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(keys[seg[g]] >> 32);
+    atomicAdd(&cnt_out[rows[q]], 1);
   }
 }
 
@@ -448,54 +514,97 @@ __global__ void k_rows_count64(const int* __restrict__ rows, int m, const long l
     out[q] = v[rows[q]] - sub;
 }
 
-static void rap_fill_sorted(const CSR& R, const CSR& A, const CSR& P, const int* rows, int m,
-                            const long long* ub, const long long* exact, CSR& Ac,
-                            cudaStream_t s) {
-  // product offsets (ub counts the diagonal seed)
-  DBuf<long long> poff((size_t)m + 1, s), rowseg((size_t)m + 1, s);
+__global__ void k_hub_pair_counts(const int* __restrict__ ria, const int* __restrict__ rows, int m,
+                                  long long* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    out[q] = 1 + ria[rows[q] + 1] - ria[rows[q]];
+}
+__global__ void k_zero_rows(const int* __restrict__ rows, int m, int* __restrict__ cnt) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    cnt[rows[q]] = 0;
+}
+__global__ void k_rows_seglen(const int* __restrict__ rows, int m, const int* __restrict__ cia,
+                              long long* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x)
+    out[q] = cia[rows[q] + 1] - cia[rows[q]];
+}
+
+struct HubStream {
+  int m = 0;
+  long long T = 0, nseg = 0;
+  DBuf<unsigned long long> keys2;
+  DBuf<long long> idx2, seg;
+  DBuf<double> vals;
+};
+
+// Phase 1 (before the scan): build and sort the streams, count columns.
+static void hub_prepare(const CSR& R, const CSR& A, const CSR& P, const int* rows, int m,
+                        int* cnt_out, HubStream& H, cudaStream_t s) {
+  H.m = m;
+  // pairs: per row 1 seed + |R row|
+  DBuf<long long> pstart((size_t)m + 1, s);
+  pstart.zero();
+  BN_LAUNCH(k_hub_pair_counts, grid_for(m, 128), 128, 0, s, R.ia.p, rows, m, pstart.p);
+  const long long npairs = scan_counts64(pstart.p, m, s);
+  DBuf<int> pair_row(npairs, s), pair_k1(npairs, s);
+  BN_LAUNCH(k_pairs, grid_for(m, 128), 128, 0, s, R.ia.p, rows, m, pstart.p, pair_row.p,
+            pair_k1.p);
+  DBuf<long long> poff((size_t)npairs + 1, s);
   poff.zero();
-  rowseg.zero();
-  BN_LAUNCH(k_rows_count64, grid_for(m, 128), 128, 0, s, rows, m, ub, 0LL, poff.p);
-  const long long T = scan_counts64(poff.p, m, s);
-  BN_LAUNCH(k_rows_count64, grid_for(m, 128), 128, 0, s, rows, m, exact, 0LL, rowseg.p);
-  const long long nseg_expect = scan_counts64(rowseg.p, m, s);
-  DBuf<unsigned long long> keys(T, s), keys2(T, s);
-  DBuf<long long> idx(T, s), idx2(T, s);
-  DBuf<double> vals(T, s);
-  BN_LAUNCH(k_rap_gen_stream, grid_for((long long)m * 32, 128), 128, 0, s, R.ia.p, R.ja.p,
-            R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, rows, m, poff.p, keys.p,
-            idx.p, vals.p);
+  BN_LAUNCH(k_pair_counts, grid_for(npairs * 32, 256), 256, 0, s, R.ia.p, R.ja.p, A.ia.p, A.ja.p,
+            P.ia.p, pair_row.p, pair_k1.p, npairs, poff.p);
+  H.T = scan_counts64(poff.p, (int)npairs, s);
+  const long long T = H.T;
+  DBuf<unsigned long long> keys(T, s);
+  DBuf<long long> idx(T, s);
+  H.keys2.alloc(T, s);
+  H.idx2.alloc(T, s);
+  H.vals.alloc(T, s);
+  BN_LAUNCH(k_rap_gen_stream, grid_for(npairs * 32, 256), 256, 0, s, R.ja.p, R.val.p, A.ia.p,
+            A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, rows, pair_row.p, pair_k1.p, npairs, poff.p,
+            keys.p, idx.p, H.vals.p);
   int eb = 33;
   while ((1LL << (eb - 32)) < (long long)m) eb++;
   size_t tmp = 0;
-  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, keys2.p, idx.p, idx2.p, T, 0, eb,
-                                          s));
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys.p, H.keys2.p, idx.p, H.idx2.p, T, 0,
+                                          eb, s));
   DBuf<unsigned char> tb(tmp, s);
-  BN_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, keys.p, keys2.p, idx.p, idx2.p, T, 0, eb, s));
-  // segment heads -> segment starts
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, keys.p, H.keys2.p, idx.p, H.idx2.p, T, 0, eb,
+                                          s));
   DBuf<unsigned char> head(T, s);
-  DBuf<long long> iota(T, s), seg(T, s), nsel(1, s);
-  BN_LAUNCH(k_seg_heads, grid_for(T, 256), 256, 0, s, keys2.p, T, head.p);
+  DBuf<long long> iota(T, s), nsel(1, s);
+  H.seg.alloc(T, s);
+  BN_LAUNCH(k_seg_heads, grid_for(T, 256), 256, 0, s, H.keys2.p, T, head.p);
   BN_LAUNCH(k_iota64, grid_for(T, 256), 256, 0, s, iota.p, T);
   tmp = 0;
-  BN_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, iota.p, head.p, seg.p, nsel.p, T, s));
+  BN_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, iota.p, head.p, H.seg.p, nsel.p, T, s));
   DBuf<unsigned char> tb2(tmp, s);
-  BN_CUDA(cub::DeviceSelect::Flagged(tb2.p, tmp, iota.p, head.p, seg.p, nsel.p, T, s));
-  const long long nseg = read_scalar(nsel.p, s);
-  BN_REQUIRE(nseg == nseg_expect, BN_ERR_ARG, "RAP: hub-row column count mismatch");
+  BN_CUDA(cub::DeviceSelect::Flagged(tb2.p, tmp, iota.p, head.p, H.seg.p, nsel.p, T, s));
+  H.nseg = read_scalar(nsel.p, s);
+  BN_LAUNCH(k_zero_rows, grid_for(m, 128), 128, 0, s, rows, m, cnt_out);
+  BN_LAUNCH(k_seg_row_counts, grid_for(H.nseg, 256), 256, 0, s, H.keys2.p, H.seg.p, H.nseg, rows,
+            cnt_out);
+}
+
+// Phase 2 (after the scan): ordered sums, reorder by first position, write.
+static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
+  const long long nseg = H.nseg, T = H.T;
+  const int m = H.m;
+  DBuf<long long> rowseg((size_t)m + 1, s);
+  rowseg.zero();
+  BN_LAUNCH(k_rows_seglen, grid_for(m, 128), 128, 0, s, rows, m, Ac.ia.p, rowseg.p);
+  scan_counts64(rowseg.p, m, s);
   DBuf<double> sval(nseg, s);
   DBuf<int> scol(nseg, s);
   DBuf<long long> sfirst(nseg, s), sfirst2(nseg, s), g_in(nseg, s), g_out(nseg, s);
   DBuf<unsigned long long> srow(nseg, s);
-  BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, keys2.p, idx2.p, vals.p, seg.p, nseg, T,
-            sval.p, scol.p, sfirst.p);
-  BN_LAUNCH(k_seg_rowkeys, grid_for(nseg, 256), 256, 0, s, keys2.p, seg.p, nseg, srow.p);
-  // order the columns of every row by first stream position (rows stay in
-  // order because their stream ranges are increasing)
+  BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, H.keys2.p, H.idx2.p, H.vals.p, H.seg.p,
+            nseg, T, sval.p, scol.p, sfirst.p);
+  BN_LAUNCH(k_seg_rowkeys, grid_for(nseg, 256), 256, 0, s, H.keys2.p, H.seg.p, nseg, srow.p);
   BN_LAUNCH(k_iota64, grid_for(nseg, 256), 256, 0, s, g_in.p, nseg);
   int fb = 1;
   while ((1LL << fb) <= T) fb++;
-  tmp = 0;
+  size_t tmp = 0;
   BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, sfirst.p, sfirst2.p, g_in.p, g_out.p, nseg,
                                           0, fb, s));
   DBuf<unsigned char> tb3(tmp, s);
@@ -566,24 +675,40 @@ static void classify(const long long* est, int nc, RapClasses& rc, cudaStream_t 
 
 void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
   const int nc = R.n;
-  {
-    BN_CUDA(cudaFuncSetAttribute(k_rap_fill_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kWarpFillSmem));
-    BN_CUDA(cudaFuncSetAttribute(k_rap_fill_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kBigFillSmem));
-    BN_CUDA(cudaFuncSetAttribute(k_rap_count_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kBigCountSmem));
-  }
-  DBuf<long long> ub(nc > 0 ? nc : 1, s);
-  DBuf<int> cnt((size_t)nc + 1, s);
+  BN_CUDA(cudaFuncSetAttribute(k_rap_fill_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kWarpFillSmem));
+  BN_CUDA(cudaFuncSetAttribute(k_rap_fill_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kBigFillSmem));
+  BN_CUDA(cudaFuncSetAttribute(k_rap_count_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kBigCountSmem));
+  DBuf<long long> ub(nc > 0 ? nc : 1, s), est(nc > 0 ? nc : 1, s);
+  DBuf<int> cnt((size_t)nc + 1, s), hub(nc > 0 ? nc : 1, s), nh(1, s);
   cnt.zero();
-  if (nc > 0)
+  nh.zero();
+  if (nc > 0) {
     BN_LAUNCH(k_rap_bound, grid_for((long long)nc * 32, 256, 16), 256, 0, s, R.ia.p, R.ja.p,
               A.ia.p, A.ja.p, P.ia.p, nc, ub.p);
-  // ---- pass 1: count, classified by min(bound, nc)
+    BN_LAUNCH(k_rap_split_hubs, grid_for(nc, 256), 256, 0, s, ub.p, ub.p, nc, est.p, hub.p, nh.p);
+  }
+  const int nhub = read_scalar(nh.p, s);
+  if (nhub > 1) {  // deterministic hub order
+    DBuf<int> t_out(nhub, s);
+    size_t tmp = 0;
+    BN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, hub.p, t_out.p, nhub, 0, 32, s));
+    DBuf<unsigned char> t(tmp, s);
+    BN_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, hub.p, t_out.p, nhub, 0, 32, s));
+    BN_CUDA(cudaMemcpyAsync(hub.p, t_out.p, sizeof(int) * nhub, cudaMemcpyDeviceToDevice, s));
+  }
+  HubStream H;
+  // ---- pass 1: count; hub rows from their sorted streams, the rest
+  // classified by min(bound, nc)
+  if (nhub > 0) {
+    Phase ph("rap hub streams", s);
+    hub_prepare(R, A, P, hub.p, nhub, cnt.p, H, s);
+  }
   {
     RapClasses rc;
-    classify(ub.p, nc, rc, s);
+    classify(est.p, nc, rc, s);
     const int* L0 = rc.lists.p;
     const int* L1 = rc.lists.p + nc;
     const int* L2 = rc.lists.p + 2 * (size_t)nc;
@@ -614,16 +739,16 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
   Ac.ia = std::move(cnt);
   Ac.ja.alloc((size_t)(nnz > 0 ? nnz : 1), s);
   Ac.val.alloc((size_t)(nnz > 0 ? nnz : 1), s);
-  // ---- pass 2: fill (hub rows by the sort path, the rest by lane-0 streams)
+  // ---- pass 2: fill
+  if (nhub > 0) {
+    Phase ph("rap hub fill", s);
+    hub_finish(hub.p, H, Ac, s);
+  }
   {
-    DBuf<long long> est(nc > 0 ? nc : 1, s);
-    DBuf<int> hub(nc > 0 ? nc : 1, s), nh(1, s);
-    nh.zero();
+    nh.zero();  // the hub list is rebuilt (and no longer needed)
     if (nc > 0)
       BN_LAUNCH(k_rap_split_hubs, grid_for(nc, 256), 256, 0, s, ub.p, exact.p, nc, est.p, hub.p,
                 nh.p);
-    const int nhub = read_scalar(nh.p, s);
-    if (nhub > 0) rap_fill_sorted(R, A, P, hub.p, nhub, ub.p, exact.p, Ac, s);
     RapClasses rc;
     classify(est.p, nc, rc, s);
     const int* L0 = rc.lists.p;

@@ -11,6 +11,8 @@
 // whose nonzeros exceed the shared buffer fall back to a per-thread walk.
 #include "solve_kernels.cuh"
 
+#include <cub/cub.cuh>
+
 namespace bn {
 
 template <class T> __device__ __forceinline__ T dmul(T a, T b);
@@ -28,7 +30,7 @@ template <class T, int MODE, bool DOT>
 __global__ void __launch_bounds__(kRows)
 k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
        const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
-       const T* __restrict__ dw, double* __restrict__ partial) {
+       const T* __restrict__ dw, double* __restrict__ partial, int skip_long) {
   __shared__ T prod[kTileNnz];
   __shared__ double red[kRows / 32];
   double dot = 0.0;
@@ -49,6 +51,7 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
       }
       __syncthreads();
     } else if (i < r1) {
+      if (skip_long && ia[i + 1] - ia[i] > kLongRow) continue;  // long-row kernel
       if (MODE == SPMV_RES) hold = b[i];
       if (MODE == SPMV_ADD) hold = y[i];
       for (int k = ia[i]; k < ia[i + 1]; k++) {
@@ -73,30 +76,142 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
   }
 }
 
-template <class T>
-void spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
-          const T* dot_w, double* partial) {
-  if (A.n == 0) return;
-  int grid = spmv_grid(A.n);
-  if (dot_w) {
-    BN_LAUNCH((k_spmv<T, SPMV_Y, true>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dot_w,
-              partial);
-    return;
+// Group-per-row SpMV for the denser coarse operators: G lanes stride a row
+// (coalesced within the group) and combine with a fixed shuffle tree.
+template <class T, int G, int MODE, bool DOT>
+__global__ void __launch_bounds__(256)
+k_spmv_vec(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+           const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
+           const T* __restrict__ dw, double* __restrict__ partial, int skip_long) {
+  __shared__ double red[8];
+  const int gl = threadIdx.x & (G - 1);
+  unsigned gmask = 0xffffffffu;
+  if constexpr (G < 32) gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+  const int groups = (gridDim.x * blockDim.x) / G;
+  double dot = 0.0;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < n; i += groups) {
+    const int k0 = ia[i], k1 = ia[i + 1];
+    if (skip_long && k1 - k0 > kLongRow) continue;  // long-row kernel
+    T sum = T(0);
+    for (int k = k0 + gl; k < k1; k += G) sum = dadd(sum, dmul(a[k], x[ja[k]]));
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) sum = dadd(sum, __shfl_xor_sync(gmask, sum, off, G));
+    if (gl == 0) {
+      T v = sum;
+      if (MODE == SPMV_RES) v = dsub(b[i], sum);
+      if (MODE == SPMV_ADD) v = dadd(y[i], sum);
+      y[i] = v;
+      if (DOT) dot += (double)dw[i] * (double)v;
+    }
   }
-  switch (mode) {
-    case SPMV_Y:
-      BN_LAUNCH((k_spmv<T, SPMV_Y, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
-                nullptr, nullptr);
+  if (DOT) {
+    for (int off = 16; off > 0; off >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; w++) t += red[w];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+// One block per long row.
+template <class T, int MODE, bool DOT>
+__global__ void __launch_bounds__(kLongThreads)
+k_spmv_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+            const T* __restrict__ x, const int* __restrict__ lrows, const T* __restrict__ b,
+            T* __restrict__ y, const T* __restrict__ dw, double* __restrict__ partial) {
+  __shared__ T red[kLongThreads / 32];
+  const int i = lrows[blockIdx.x];
+  T sum = T(0);
+  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += kLongThreads)
+    sum = dadd(sum, dmul(a[k], x[ja[k]]));
+  for (int off = 16; off > 0; off >>= 1) sum = dadd(sum, __shfl_xor_sync(0xffffffffu, sum, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T t = T(0);
+    for (int w = 0; w < kLongThreads / 32; w++) t = dadd(t, red[w]);
+    T v = t;
+    if (MODE == SPMV_RES) v = dsub(b[i], t);
+    if (MODE == SPMV_ADD) v = dadd(y[i], t);
+    y[i] = v;
+    if (DOT) partial[blockIdx.x] = (double)dw[i] * (double)v;
+  }
+}
+
+__global__ void k_long_rows(const int* __restrict__ ia, int n, int* __restrict__ lrows,
+                            int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (ia[i + 1] - ia[i] > kLongRow) lrows[atomicAdd(counter, 1)] = i;
+}
+
+void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {
+  const double avg = A.n > 0 ? (double)A.nnz / A.n : 0.0;
+  out.group = avg <= 8.0 ? 0 : (avg <= 16.0 ? 4 : (avg <= 48.0 ? 8 : 32));
+  DBuf<int> cnt(1, s);
+  cnt.zero();
+  out.lrows.alloc(A.n > 0 ? A.n : 1, s);
+  if (A.n > 0)
+    BN_LAUNCH(k_long_rows, grid_for(A.n, 256), 256, 0, s, A.ia.p, A.n, out.lrows.p, cnt.p);
+  out.nlong = read_scalar(cnt.p, s);
+  if (out.nlong > 1) {  // deterministic order
+    DBuf<int> tmp_out(out.nlong, s);
+    size_t tmp = 0;
+    BN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, out.lrows.p, tmp_out.p, out.nlong, 0, 32, s));
+    DBuf<unsigned char> t(tmp, s);
+    BN_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, out.lrows.p, tmp_out.p, out.nlong, 0, 32, s));
+    BN_CUDA(cudaMemcpyAsync(out.lrows.p, tmp_out.p, sizeof(int) * out.nlong,
+                            cudaMemcpyDeviceToDevice, s));
+    BN_CUDA(cudaStreamSynchronize(s));
+  }
+}
+
+int spmv_partials(int n, int nlong) { return spmv_grid(n) + nlong; }
+
+template <class T, int MODE, bool DOT>
+static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
+                          const T* dw, double* partial) {
+  const int grid = spmv_grid(A.n);
+  const int skip = A.lrows != nullptr ? 1 : 0;
+  switch (A.group) {
+    case 0:
+      BN_LAUNCH((k_spmv<T, MODE, DOT>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dw,
+                partial, skip);
       break;
-    case SPMV_RES:
-      BN_LAUNCH((k_spmv<T, SPMV_RES, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
-                nullptr, nullptr);
+    case 4:
+      BN_LAUNCH((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip);
+      break;
+    case 8:
+      BN_LAUNCH((k_spmv_vec<T, 8, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip);
       break;
     default:
-      BN_LAUNCH((k_spmv<T, SPMV_ADD, false>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
-                nullptr, nullptr);
+      BN_LAUNCH((k_spmv_vec<T, 32, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip);
       break;
   }
+  if (A.nlong > 0)
+    BN_LAUNCH((k_spmv_long<T, MODE, DOT>), A.nlong, kLongThreads, 0, s, A.ia, A.ja, A.val, x,
+              A.lrows, b, y, dw, DOT ? partial + grid : nullptr);
+}
+
+template <class T>
+int spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
+         const T* dot_w, double* partial) {
+  if (A.n == 0) return 0;
+  if (dot_w) {
+    spmv_dispatch<T, SPMV_Y, true>(A, x, b, y, s, dot_w, partial);
+    return spmv_partials(A.n, A.nlong);
+  }
+  switch (mode) {
+    case SPMV_Y: spmv_dispatch<T, SPMV_Y, false>(A, x, b, y, s, nullptr, nullptr); break;
+    case SPMV_RES: spmv_dispatch<T, SPMV_RES, false>(A, x, b, y, s, nullptr, nullptr); break;
+    default: spmv_dispatch<T, SPMV_ADD, false>(A, x, b, y, s, nullptr, nullptr); break;
+  }
+  return 0;
 }
 
 // ----------------------------------------------------- coloured Gauss-Seidel
@@ -141,6 +256,35 @@ __global__ void k_gs_color(const int* __restrict__ ia, const int* __restrict__ j
   }
 }
 
+// one block per long row of a colour class
+template <class T>
+__global__ void __launch_bounds__(kLongThreads)
+k_gs_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+          const int* __restrict__ rows, const T* __restrict__ b, T* x, T* __restrict__ out) {
+  __shared__ T red[kLongThreads / 32];
+  __shared__ T dsh;
+  __shared__ int has;
+  const int t = blockIdx.x;
+  const int i = rows[t];
+  if (threadIdx.x == 0) { has = 0; dsh = T(1); }
+  __syncthreads();
+  T sum = T(0);
+  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += kLongThreads) {
+    const int j = ja[k];
+    if (j == i) { dsh = a[k]; has = 1; }
+    else sum = dadd(sum, dmul(a[k], x[j]));
+  }
+  for (int off = 16; off > 0; off >>= 1) sum = dadd(sum, __shfl_xor_sync(0xffffffffu, sum, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T s = T(0);
+    for (int w = 0; w < kLongThreads / 32; w++) s = dadd(s, red[w]);
+    const T xi = dsub(b[i], s) / (has ? dsh : T(1));
+    if (out) out[t] = xi; else x[i] = xi;
+  }
+}
+
 template <class T>
 __global__ void k_scatter(const int* __restrict__ rows, int nr, const T* __restrict__ v,
                           T* __restrict__ x) {
@@ -150,7 +294,14 @@ __global__ void k_scatter(const int* __restrict__ rows, int nr, const T* __restr
 
 template <class T>
 static void gs_launch(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* out,
-                      int group, cudaStream_t s) {
+                      int group, cudaStream_t s, int nlong = 0) {
+  // the last nlong rows of the class are long rows: one block each
+  if (nlong > 0) {
+    BN_LAUNCH(k_gs_long<T>, nlong, kLongThreads, 0, s, A.ia, A.ja, A.val, rows + (nr - nlong), b,
+              x, out ? out + (nr - nlong) : nullptr);
+    nr -= nlong;
+    if (nr == 0) return;
+  }
   if (group >= 32)
     BN_LAUNCH((k_gs_color<T, 32>), grid_for((long long)nr * 32, 256, 8), 256, 0, s, A.ia, A.ja,
               A.val, rows, nr, b, x, out);
@@ -164,16 +315,16 @@ static void gs_launch(const DevMat<T>& A, const int* rows, int nr, const T* b, T
 
 template <class T>
 void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
-              cudaStream_t s) {
+              cudaStream_t s, int nlong) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, nr, b, x, nullptr, group, s);
+  gs_launch<T>(A, rows, nr, b, x, nullptr, group, s, nlong);
 }
 
 template <class T>
 void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
-                  int group, cudaStream_t s) {
+                  int group, cudaStream_t s, int nlong) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, nr, b, x, tmp, group, s);
+  gs_launch<T>(A, rows, nr, b, x, tmp, group, s, nlong);
   BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, nr, tmp, x);
 }
 
@@ -309,12 +460,12 @@ void pcg_scalars(double* sc, int flexible, cudaStream_t s) {
 
 // explicit instantiations
 #define BN_INST(T)                                                                           \
-  template void spmv<T>(int, const DevMat<T>&, const T*, const T*, T*, cudaStream_t, const T*, \
-                        double*);                                                            \
+  template int spmv<T>(int, const DevMat<T>&, const T*, const T*, T*, cudaStream_t, const T*,  \
+                       double*);                                                             \
   template void gs_color<T>(const DevMat<T>&, const int*, int, const T*, T*, int,            \
-                            cudaStream_t);                                                   \
+                            cudaStream_t, int);                                              \
   template void jacobi_class<T>(const DevMat<T>&, const int*, int, const T*, T*, T*, int,     \
-                                cudaStream_t);                                               \
+                                cudaStream_t, int);                                          \
   template void vzero<T>(T*, int, cudaStream_t);                                             \
   template void vadd<T>(const T*, const T*, int, T*, cudaStream_t);                          \
   template void dot_partials<T>(const T*, const T*, const T*, int, double*, double*,          \

@@ -24,14 +24,31 @@ enum ScalarSlot : int {
   SC_COUNT = 16
 };
 
-// Non-owning CSR view with values of type T.
+constexpr int kLongRow = 1024;    // rows longer than this get a block each
+constexpr int kLongThreads = 256;
+
+// Non-owning CSR view with values of type T, plus the row-length layout the
+// kernels dispatch on: group == 0 selects the row-tile kernel (short rows),
+// otherwise `group` lanes per row; rows longer than kLongRow are listed in
+// lrows and handled by one block each.
 template <class T>
 struct DevMat {
   int n = 0, m = 0, nnz = 0;
   const int* ia = nullptr;
   const int* ja = nullptr;
   const T* val = nullptr;
+  int group = 0;
+  const int* lrows = nullptr;
+  int nlong = 0;
 };
+
+// Row-length layout of a CSR matrix (computed once at setup).
+struct RowLayout {
+  int group = 0;
+  DBuf<int> lrows;
+  int nlong = 0;
+};
+void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s);
 
 inline int spmv_grid(int n) {
   int tiles = (n + kRows - 1) / kRows;
@@ -39,15 +56,19 @@ inline int spmv_grid(int n) {
   return tiles < cap ? tiles : cap;
 }
 
+// y = A x | b - A x | y + A x.  With dot_w, also writes partial sums of
+// dot_w . y; returns the number of partial slots written (0 without dot_w).
 template <class T>
-void spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
-          const T* dot_w = nullptr, double* partial = nullptr);
+int spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
+         const T* dot_w = nullptr, double* partial = nullptr);
+int spmv_partials(int n, int nlong);
+// rows of one colour class; its last nlong rows are long rows (block each)
 template <class T>
 void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
-              cudaStream_t s);
+              cudaStream_t s, int nlong = 0);
 template <class T>
 void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
-                  int group, cudaStream_t s);
+                  int group, cudaStream_t s, int nlong = 0);
 template <class T>
 void vzero(T* x, int n, cudaStream_t s);
 template <class TO, class TI>

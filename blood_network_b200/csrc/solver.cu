@@ -32,8 +32,9 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
   return x;
 }
 
-// Jones-Plassmann-Luby rounds with first-fit colours: an uncoloured row
-// whose priority beats every uncoloured neighbour of its own set takes the
+// Jones-Plassmann-Luby rounds with first-fit colours (largest-degree-first
+// priorities): an uncoloured row whose priority beats every uncoloured
+// neighbour of its own set takes the
 // smallest colour that no already-coloured neighbour of its set holds.
 // Rows selected in one round are never adjacent, so the colouring is
 // proper.  Colours are capped at kMaxColors per set; a row that finds all
@@ -48,7 +49,9 @@ __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     newc[i] = -1;
     if (color[i] >= 0) continue;
-    const unsigned hi = color_hash((unsigned)i);
+    // priority: row length first (dense rows decide early), hash second
+    const unsigned long long pi =
+        ((unsigned long long)(ia[i + 1] - ia[i]) << 32) | color_hash((unsigned)i);
     const int si = set ? set[i] : 0;
     bool is_max = true;
     unsigned used = 0;
@@ -59,7 +62,7 @@ __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict_
       const int cj = color[j];
       if (cj >= 0) {
         if (cj < kMaxColors) used |= 1u << cj;
-      } else if (color_hash((unsigned)j) > hi) {
+      } else if ((((unsigned long long)(ia[j + 1] - ia[j]) << 32) | color_hash((unsigned)j)) > pi) {
         is_max = false;
         break;
       }
@@ -77,11 +80,13 @@ __global__ void k_color_commit(int n, const int* __restrict__ newc, int* __restr
     if (newc[i] >= 0) color[i] = newc[i];
 }
 
-// key = set * 64 + colour ; C points are set 0, F points set 1
-__global__ void k_color_keys(const int* __restrict__ set, const int* __restrict__ color, int n,
-                             int* __restrict__ key, int* __restrict__ ids) {
+// key = ((set * 64 + colour) << 1) | long ; C points are set 0, F points
+// set 1; long rows sort to the end of their class
+__global__ void k_color_keys(const int* __restrict__ set, const int* __restrict__ color,
+                             const int* __restrict__ ia, int n, int* __restrict__ key,
+                             int* __restrict__ ids) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    key[i] = (set ? set[i] : 0) * 64 + color[i];
+    key[i] = (((set ? set[i] : 0) * 64 + color[i]) << 1) | (ia[i + 1] - ia[i] > kLongRow ? 1 : 0);
     ids[i] = i;
   }
 }
@@ -128,6 +133,7 @@ __global__ void k_to_f32(const double* __restrict__ a, size_t m, T* __restrict__
 // ------------------------------------------------------------ data
 struct Level {
   CSR A, S, P, R;
+  RowLayout layA, layP, layR;  // SpMV row-length layouts
   DBuf<int> cf;
   int n_coarse = 0;
   int max_lam = 0;
@@ -136,6 +142,7 @@ struct Level {
   DBuf<int> gs_rows;
   std::vector<int> cptr;   // colour class offsets into gs_rows
   std::vector<char> cjac;  // class is an overflow class (Jacobi update)
+  std::vector<int> clong;  // long rows at the end of each class
   int colored_for = -1;    // smoother the colouring was built for
   int color_rounds = 0;
   int gs_group = 1;        // lanes per row in the GS kernel
@@ -153,6 +160,7 @@ struct Solver {
   std::vector<std::unique_ptr<Level>> lv;
   DenseCoarse coarse;
   CSR Aown;               // solve matrix when set_matrix replaced it
+  RowLayout layOwn;
   bool own_solve = false;
   DBuf<float> Aown32;
   IChol ic;
@@ -179,7 +187,9 @@ struct Solver {
   void color_level(Level& L, int smoother);
   void alloc_vectors();
   void drop_graphs();
-  template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32) const;
+  template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32,
+                                   const RowLayout* lay) const;
+  const RowLayout& lay_solve() const { return own_solve ? layOwn : lv[0]->layA; }
   template <class T> void smooth(int l, const T* bb, T* xl, bool forward);
   template <class T> void backslash(int l, const T* bb, T* xl);
   template <class T> void fwdslash(int l, const T* bb, T* xl);
@@ -201,11 +211,12 @@ void Solver::drop_graphs() {
 }
 
 template <class T>
-DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32) const {
+DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32, const RowLayout* lay) const {
   DevMat<T> d;
   d.n = M.n; d.m = M.m; d.nnz = M.nnz; d.ia = M.ia.p; d.ja = M.ja.p;
   if constexpr (sizeof(T) == 8) d.val = M.val.p;
   else d.val = v32->p;
+  if (lay) { d.group = lay->group; d.lrows = lay->lrows.p; d.nlong = lay->nlong; }
   return d;
 }
 
@@ -231,23 +242,29 @@ void Solver::color_level(Level& L, int smoother) {
   }
   DBuf<int> key(n, s), ids(n, s), key_out(n, s);
   L.gs_rows.alloc(n, s);
-  BN_LAUNCH(k_color_keys, g, 256, 0, s, cf_split ? set.p : nullptr, color.p, n, key.p, ids.p);
+  BN_LAUNCH(k_color_keys, g, 256, 0, s, cf_split ? set.p : nullptr, color.p, L.A.ia.p, n, key.p,
+            ids.p);
   size_t tmp = 0;
   BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n,
-                                          0, 7, s));
+                                          0, 8, s));
   DBuf<unsigned char> t(tmp, s);
-  BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n, 0, 7,
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n, 0, 8,
                                           s));
   std::vector<int> hk(n);
   key_out.download(hk.data(), n);
   BN_CUDA(cudaStreamSynchronize(s));
   L.cptr.clear();
   L.cjac.clear();
+  L.clong.clear();
   L.cptr.push_back(0);
+  int nlong = 0;
   for (int i = 1; i <= n; i++) {
-    if (i == n || hk[i] != hk[i - 1]) {
+    nlong += (hk[i - 1] & 1);
+    if (i == n || (hk[i] >> 1) != (hk[i - 1] >> 1)) {
       L.cptr.push_back(i);
-      L.cjac.push_back((hk[i - 1] & 63) == kMaxColors ? 1 : 0);
+      L.cjac.push_back(((hk[i - 1] >> 1) & 63) == kMaxColors ? 1 : 0);
+      L.clong.push_back(nlong);
+      nlong = 0;
     }
   }
   L.colored_for = smoother;
@@ -275,7 +292,8 @@ void Solver::alloc_vectors() {
     for (auto* v : {&g32, &u1f, &r1f, &icyf, &icxf, &xxf, &r2f, &corrf}) v->alloc(n0, s);
   sc.alloc(SC_COUNT, s);
   sc.zero();
-  part0.alloc(kRedBlocks > spmv_grid(n0) ? kRedBlocks : spmv_grid(n0), s);
+  const int np = spmv_partials(n0, lay_solve().nlong);
+  part0.alloc(kRedBlocks > np ? kRedBlocks : np, s);
   part1.alloc(kRedBlocks, s);
   if (!h_sc) BN_CUDA(cudaMallocHost((void**)&h_sc, sizeof(double) * SC_COUNT));
 }
@@ -315,6 +333,18 @@ void Solver::prepare_f32() {
 void Solver::finish_setup() {
   const int nl = (int)lv.size();
   { Phase ph("dense coarse", s, nl - 1); coarse.setup(lv[nl - 1]->A, s); }
+  {
+    Phase ph("row layouts", s);
+    for (int l = 0; l < nl; l++) {
+      Level& L = *lv[l];
+      analyze_rows(L.A, L.layA, s);
+      if (l < nl - 1) {
+        analyze_rows(L.P, L.layP, s);
+        analyze_rows(L.R, L.layR, s);
+      }
+    }
+    if (own_solve) analyze_rows(Aown, layOwn, s);
+  }
   for (int l = 0; l < nl - 1; l++) {
     Level& L = *lv[l];
     const int sm = opt.smoother;
@@ -409,7 +439,7 @@ template <class T>
 void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
   Level& L = *lv[l];
   const bool f64 = sizeof(T) == 8;
-  DevMat<T> A = mat<T>(L.A, &L.A32);
+  DevMat<T> A = mat<T>(L.A, &L.A32, &L.layA);
   const int n = L.A.n;
   for (int sweep = 0; sweep < opt.nu; sweep++) {
     switch (opt.smoother) {
@@ -422,9 +452,9 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
           const int* rows = L.gs_rows.p + L.cptr[c];
           const int nr = L.cptr[c + 1] - L.cptr[c];
           if (L.cjac[c])
-            jacobi_class<T>(A, rows, nr, bb, xl, tmp, L.gs_group, s);
+            jacobi_class<T>(A, rows, nr, bb, xl, tmp, L.gs_group, s, L.clong[c]);
           else
-            gs_color<T>(A, rows, nr, bb, xl, L.gs_group, s);
+            gs_color<T>(A, rows, nr, bb, xl, L.gs_group, s, L.clong[c]);
         }
         break;
       }
@@ -461,11 +491,11 @@ void Solver::backslash(int l, const T* bb, T* xl) {
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
   { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
-  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.A, &L.A32), xl, bb, rr, s); }
-  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32), rr, nullptr, cb, s); }
+  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.A, &L.A32, &L.layA), xl, bb, rr, s); }
+  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32, &L.layR), rr, nullptr, cb, s); }
   if (l + 1 < nl - 1) vzero<T>(cx, C.A.n, s);
   backslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_ADD, mat<T>(L.P, &L.P32), cx, nullptr, xl, s);  // x += P ec
+  spmv<T>(SPMV_ADD, mat<T>(L.P, &L.P32, &L.layP), cx, nullptr, xl, s);  // x += P ec
 }
 
 // fwdslash_rec (amg_cycle.c:222-253); xl is zero on entry, so the first
@@ -482,9 +512,9 @@ void Solver::fwdslash(int l, const T* bb, T* xl) {
   const bool f64 = sizeof(T) == 8;
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
-  spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32), bb, nullptr, cb, s);  // rc = P^T b
+  spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32, &L.layR), bb, nullptr, cb, s);  // rc = P^T b
   fwdslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_Y, mat<T>(L.P, &L.P32), cx, nullptr, xl, s);  // x = P ec
+  spmv<T>(SPMV_Y, mat<T>(L.P, &L.P32, &L.layP), cx, nullptr, xl, s);  // x = P ec
   smooth<T>(l, bb, xl, false);
 }
 
@@ -501,7 +531,7 @@ void Solver::precond_t(const T* g, T* out) {
   T* XX = f64 ? (T*)xx.p : (T*)xxf.p;
   T* R2 = f64 ? (T*)r2.p : (T*)r2f.p;
   T* CO = f64 ? (T*)corr.p : (T*)corrf.p;
-  DevMat<T> As = own_solve ? mat<T>(Aown, &Aown32) : mat<T>(lv[0]->A, &lv[0]->A32);
+  DevMat<T> As = own_solve ? mat<T>(Aown, &Aown32, &layOwn) : mat<T>(lv[0]->A, &lv[0]->A32, &lv[0]->layA);
   vzero<T>(U1, n0, s);
   { Phase ph("backslash", s); backslash<T>(0, g, U1); }
   { Phase ph("residual r1", s); spmv<T>(SPMV_RES, As, U1, g, R1, s); }
@@ -560,8 +590,7 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   const int n0 = n();
   const bool flexible = (opt.precision == AMG_PREC_MIXED);
   if (flexible && !f32_ready) prepare_f32();
-  DevMat<double> A = mat<double>(Asolve(), nullptr);
-  const int sg = spmv_grid(n0);
+  DevMat<double> A = mat<double>(Asolve(), nullptr, &lay_solve());
   cudaEventRecord(ev0, s);
   BN_CUDA(cudaMemcpyAsync(b.p, d_b, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
   BN_CUDA(cudaMemcpyAsync(x.p, d_x, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
@@ -590,8 +619,8 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   int iter;
   int status = BN_OK;
   for (iter = 1; iter <= maxiter; iter++) {
-    spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s, p.p, part0.p);  // Ap, p.Ap
-    reduce_partials(part0.p, sg, sc.p + SC_PAP, s);
+    int np = spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s, p.p, part0.p);  // Ap, p.Ap
+    reduce_partials(part0.p, np, sc.p + SC_PAP, s);
     pcg_update_xr(x.p, r.p, p.p, ap.p, n0, sc.p, part0.p, s);      // x, r, r.r
     reduce_partials(part0.p, kRedBlocks, sc.p + SC_RR, s);
     if (flexible) {  // r_{k+1}.z_k before z is overwritten
@@ -794,10 +823,12 @@ BN_API int amg_solver_set_matrix(void* h, int n, int nnz, const int* ia, const i
     bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
     S->Aown = std::move(A);
     S->own_solve = true;
+    bn::analyze_rows(S->Aown, S->layOwn, S->s);
     S->ic.want_f32 = (S->opt.precision == AMG_PREC_MIXED);
     S->ic.factor(S->Aown, S->s);
     S->f32_ready = false;
     if (S->opt.precision == AMG_PREC_MIXED) S->prepare_f32();
+    S->alloc_vectors();
     S->drop_graphs();
     bn::set_last_error(0, "");
     return 0;
@@ -906,6 +937,69 @@ BN_API int amg_solver_precond(void* h, const double* g, double* xo) {
     BN_CUDA(cudaStreamSynchronize(S->s));
     int e = S->ic.take_error(S->s);
     BN_REQUIRE(e == 0, e, "IC(0) solve: a bounded dependency wait ran out");
+    return 0;
+  }, bn::BN_ERR_CUDA);
+}
+
+// Times `reps` launches of one hot operation with CUDA events on the solver's
+// stream (after one untimed launch).  which: 0 fine-level residual SpMV
+// r = b - A x, 1 fine-level forward Gauss-Seidel sweep (all colour classes),
+// 2 one preconditioner application, 3 one IC(0) solve (forward + backward).
+// precision: 0 FP64, 1 FP32 (the mixed form's V-cycle copies).  Writes the
+// mean milliseconds per launch to *ms.  Inputs are the PCG's own vectors.
+BN_API int amg_solver_bench_kernel(void* h, int which, int precision, int reps, double* ms) {
+  if (!h || !ms || reps <= 0) return bn::BN_ERR_ARG;
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    const bool f32 = precision == 1;
+    if (f32 && !S->f32_ready) {
+      if (!S->ic.fval32.n) { S->ic.want_f32 = true; S->ic.refresh_values(); }
+      S->prepare_f32();
+    }
+    if (f32 && !S->g32.n) {
+      const int keep = S->opt.precision;
+      S->opt.precision = AMG_PREC_MIXED;
+      S->alloc_vectors();
+      S->opt.precision = keep;
+    }
+    const int n = S->n();
+    bn::Level& L0 = *S->lv[0];
+    auto run = [&]() {
+      switch (which) {
+        case 0:
+          if (f32)
+            bn::spmv<float>(bn::SPMV_RES, S->mat<float>(S->Asolve(), S->own_solve ? &S->Aown32 : &L0.A32,
+                                                         &S->lay_solve()),
+                            S->xxf.p, S->g32.p, S->r1f.p, S->s);
+          else
+            bn::spmv<double>(bn::SPMV_RES, S->mat<double>(S->Asolve(), nullptr, &S->lay_solve()),
+                             S->x.p, S->b.p, S->r.p, S->s);
+          break;
+        case 1:
+          if (S->lv.size() < 2) break;
+          if (f32) S->smooth<float>(0, S->g32.p, S->u1f.p, true);
+          else S->smooth<double>(0, S->b.p, S->u1.p, true);
+          break;
+        case 2:
+          S->precond(S->b.p, S->z.p);
+          break;
+        default:
+          if (f32) S->ic.solve<float>(S->g32.p, S->icyf.p, S->icxf.p, S->s);
+          else S->ic.solve<double>(S->b.p, S->icy.p, S->icx.p, S->s);
+          break;
+      }
+    };
+    run();
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    cudaEventRecord(S->ev0, S->s);
+    for (int r = 0; r < reps; r++) run();
+    cudaEventRecord(S->ev1, S->s);
+    BN_CUDA(cudaEventSynchronize(S->ev1));
+    float t = 0;
+    cudaEventElapsedTime(&t, S->ev0, S->ev1);
+    *ms = (double)t / reps;
+    (void)n;
     return 0;
   }, bn::BN_ERR_CUDA);
 }

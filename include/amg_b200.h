@@ -154,6 +154,12 @@ int amg_solver_level_copy(void* handle, int level, int* a_ia, int* a_ja, double*
                           int* s_ia, int* s_ja, double* s_val, int* p_ia, int* p_ja,
                           double* p_val, int* cf);
 
+/* Times `reps` launches of one hot operation with CUDA events on the
+ * solver's stream; *ms receives the mean milliseconds per launch.
+ * which: 0 fine residual SpMV, 1 fine forward Gauss-Seidel sweep,
+ * 2 preconditioner application, 3 IC(0) solve.  precision: 0 FP64, 1 FP32. */
+int amg_solver_bench_kernel(void* handle, int which, int precision, int reps, double* ms);
+
 const char* amg_solver_last_error(void);
 int amg_solver_last_status(void);
 unsigned long long amg_b200_launch_count(void);
