@@ -191,6 +191,33 @@ def run_reference(args):
     return 0
 
 
+# --------------------------------------------------------------- profiling driver
+def run_profile(args):
+    import torch
+    from blood_network_b200 import amg
+    from blood_network_b200.network import make_config, CONFIGS
+    cfg = CONFIGS[args.config]
+    coarsen = {"pmis": amg.COARSEN_PMIS, "hmis": amg.COARSEN_HMIS, "rs": amg.COARSEN_RS}[
+        cfg["coarsening"]]
+    net = make_config(args.config, keep_segments=False)
+    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, threshold=cfg["theta"],
+                      coarsening=coarsen, precision=amg.PREC_MIXED, stop=amg.STOP_RELRES)
+    if args.profile == "solve":
+        s.solve(net.rhs, tol=1e-8)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profiled_solve")
+        x, it = s.solve(net.rhs, tol=1e-8)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(f"profiled solve: n={net.n} nnz={net.nnz} iterations={it}", flush=True)
+    else:
+        which, prec = (0, 0) if args.profile == "spmv" else (1, 1)
+        ms = s.bench_kernel(which, prec, reps=2)
+        print(f"{args.profile}: n={net.n} nnz={net.nnz} {ms:.3f} ms/launch", flush=True)
+    s.close()
+    return 0
+
+
 # --------------------------------------------------------------- B200 arm
 def main():
     ap = argparse.ArgumentParser()
@@ -201,9 +228,15 @@ def main():
     ap.add_argument("--config", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--profile", choices=["solve", "spmv", "gs"], default=None,
+                    help="profiling driver: 'solve' runs one warm-up and one NVTX-scoped "
+                         "('profiled_solve') mixed solve; 'spmv'/'gs' run the fine-level FP64 "
+                         "residual SpMV / FP32 GS sweep three times after setup")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
     args.warmup = max(args.warmup, 3)
 
     rank, ws, local = dist_init(args)

@@ -23,6 +23,7 @@
 // waits anywhere, so nothing can spin.
 #include "ichol.cuh"
 
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 namespace bn {
@@ -226,6 +227,127 @@ k_tri_batch(const int* __restrict__ ia, const int* __restrict__ ja, const T* __r
   }
 }
 
+// Cooperative form: the whole sweep in one launch.  Segment s is either one
+// wide level spread over the grid or a run of narrow levels stepped by block
+// 0 with __syncthreads(); a grid-wide barrier separates segments.  Values of
+// earlier levels are read with ld.global.cg (L2), since another SM wrote them.
+constexpr int kCoopThreads = 256;
+constexpr int kCoopNarrow = 4 * kCoopThreads;
+
+template <class T>
+__device__ __forceinline__ void tri_row_cg(int t, const int* __restrict__ ia,
+                                           const int* __restrict__ ja, const T* __restrict__ val,
+                                           const T* __restrict__ diag,
+                                           const int* __restrict__ rows,
+                                           const T* __restrict__ in, T* x) {
+  const int i = rows[t];
+  T s = in[i];
+  for (int k = ia[t]; k < ia[t + 1]; k++) {
+    if constexpr (sizeof(T) == 8)
+      s = xsub(s, xmul(val[k], __ldcg(x + ja[k])));
+    else
+      s = xsubf(s, xmulf(val[k], __ldcg(x + ja[k])));
+  }
+  __stcg(x + i, s / diag[t]);
+}
+
+// A thread's first row of the next wide level, loaded before the grid
+// barrier: everything but the values of the dependencies (which the
+// barrier publishes) is known in advance.
+constexpr int kPre = 4;
+template <class T>
+struct RowPre {
+  int t;       // position in the layout, -1 if none
+  int i, k0, k1;
+  T in_i, d;
+  int j[kPre];
+  T v[kPre];
+};
+
+template <class T>
+__device__ __forceinline__ void pre_load(RowPre<T>& p, int t, const int* __restrict__ ia,
+                                         const int* __restrict__ ja, const T* __restrict__ val,
+                                         const T* __restrict__ diag,
+                                         const int* __restrict__ rows,
+                                         const T* __restrict__ in) {
+  p.t = t;
+  p.i = rows[t];
+  p.k0 = ia[t];
+  p.k1 = ia[t + 1];
+  p.in_i = in[p.i];
+  p.d = diag[t];
+#pragma unroll
+  for (int q = 0; q < kPre; q++) {
+    if (p.k0 + q < p.k1) {
+      p.j[q] = ja[p.k0 + q];
+      p.v[q] = val[p.k0 + q];
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void pre_finish(const RowPre<T>& p, const int* __restrict__ ja,
+                                           const T* __restrict__ val, T* x) {
+  T s = p.in_i;
+  T xv[kPre];
+#pragma unroll
+  for (int q = 0; q < kPre; q++)
+    if (p.k0 + q < p.k1) xv[q] = __ldcg(x + p.j[q]);  // independent loads in flight
+#pragma unroll
+  for (int q = 0; q < kPre; q++) {
+    if (p.k0 + q < p.k1) {
+      if constexpr (sizeof(T) == 8) s = xsub(s, xmul(p.v[q], xv[q]));
+      else s = xsubf(s, xmulf(p.v[q], xv[q]));
+    }
+  }
+  for (int k = p.k0 + kPre; k < p.k1; k++) {
+    if constexpr (sizeof(T) == 8) s = xsub(s, xmul(val[k], __ldcg(x + ja[k])));
+    else s = xsubf(s, xmulf(val[k], __ldcg(x + ja[k])));
+  }
+  __stcg(x + p.i, s / p.d);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kCoopThreads)
+k_tri_coop(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+           const T* __restrict__ diag, const int* __restrict__ rows, const int* __restrict__ lptr,
+           const int4* __restrict__ segs, int nseg, const T* __restrict__ in, T* x) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gsz = gridDim.x * blockDim.x;
+  RowPre<T> pre;
+  pre.t = -1;
+  if (nseg > 0 && segs[0].x == 0) {
+    const int t = lptr[segs[0].y] + gtid;
+    if (t < lptr[segs[0].y + 1]) pre_load<T>(pre, t, ia, ja, val, diag, rows, in);
+  }
+  for (int q = 0; q < nseg; q++) {
+    const int4 sg = segs[q];
+    if (sg.x == 0) {
+      if (pre.t >= 0) pre_finish<T>(pre, ja, val, x);
+      for (int t = lptr[sg.y] + gtid + gsz; t < lptr[sg.y + 1]; t += gsz)
+        tri_row_cg<T>(t, ia, ja, val, diag, rows, in, x);
+    } else if (blockIdx.x == 0) {
+      for (int l = sg.y; l < sg.z; l++) {
+        for (int t = lptr[l] + threadIdx.x; t < lptr[l + 1]; t += blockDim.x)
+          tri_row_cg<T>(t, ia, ja, val, diag, rows, in, x);
+        __syncthreads();
+      }
+    }
+    // prefetch this thread's first row of the next segment if it is wide
+    pre.t = -1;
+    if (q + 1 < nseg) {
+      const int4 nx = segs[q + 1];
+      if (nx.x == 0) {
+        const int t = lptr[nx.y] + gtid;
+        if (t < lptr[nx.y + 1]) pre_load<T>(pre, t, ia, ja, val, diag, rows, in);
+      }
+    }
+    grid.sync();
+  }
+}
+
 // ---------------------------------------------------------------- layout
 __global__ void k_fwd_count(const int* __restrict__ lia, const int* __restrict__ lja,
                             const int* __restrict__ order, int n, int* __restrict__ cnt) {
@@ -284,6 +406,12 @@ __global__ void k_gather_diag(const int* __restrict__ order, int n, const int* _
     out[t] = (T)lval[dpos[order[t]]];
 }
 
+__global__ void k_map_ids(const int* __restrict__ src, int m, const int* __restrict__ inv,
+                          int* __restrict__ dst) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
+    dst[p] = inv ? inv[src[p]] : src[p];
+}
+
 __global__ void k_double_to_int(const double* __restrict__ a, int m, int* __restrict__ b) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x)
     b[p] = (int)a[p];
@@ -292,22 +420,31 @@ __global__ void k_double_to_int(const double* __restrict__ a, int m, int* __rest
 // ---------------------------------------------------------------- host
 // Segments: a wide level is one grid launch; a run of narrow levels is one
 // batched block.  Built from host level offsets.
-static void make_segments(const std::vector<int>& ptr, std::vector<IChol::Seg>& segs) {
+static void make_segments(const std::vector<int>& ptr, std::vector<IChol::Seg>& segs,
+                          int narrow = kNarrow) {
   segs.clear();
   const int nl = (int)ptr.size() - 1;
   int l = 0;
   while (l < nl) {
     int w = ptr[l + 1] - ptr[l];
-    if (w > kNarrow) {
+    if (w > narrow) {
       segs.push_back({0, l, l + 1, ptr[l], ptr[l + 1]});
       l++;
     } else {
       int l1 = l;
-      while (l1 < nl && ptr[l1 + 1] - ptr[l1] <= kNarrow) l1++;
+      while (l1 < nl && ptr[l1 + 1] - ptr[l1] <= narrow) l1++;
       segs.push_back({1, l, l1, ptr[l], ptr[l1]});
       l = l1;
     }
   }
+}
+
+static void upload_segs(const std::vector<IChol::Seg>& segs, DBuf<int4>& d, cudaStream_t s) {
+  std::vector<int4> h(segs.size());
+  for (size_t q = 0; q < segs.size(); q++) h[q] = make_int4(segs[q].kind, segs[q].l0, segs[q].l1, 0);
+  d.alloc(h.size() > 0 ? h.size() : 1, s);
+  if (!h.empty()) d.upload(h.data(), h.size());
+  BN_CUDA(cudaStreamSynchronize(s));
 }
 
 void IChol::factor(const CSR& A, cudaStream_t s) {
@@ -413,6 +550,15 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   for (int l = 0; l <= nlevels; l++) bptr[l] = n - lptr[nlevels - l];
   make_segments(lptr, fseg);
   make_segments(bptr, bseg);
+  {
+    std::vector<Seg> cf, cb;
+    make_segments(lptr, cf, kCoopNarrow);
+    make_segments(bptr, cb, kCoopNarrow);
+    upload_segs(cf, d_cfseg, s);
+    upload_segs(cb, d_cbseg, s);
+    n_cfseg = (int)cf.size();
+    n_cbseg = (int)cb.size();
+  }
   d_lptr.alloc(nlevels + 1, s);
   d_lptr.upload(lptr.data(), nlevels + 1);
   d_bptr.alloc(nlevels + 1, s);
@@ -452,6 +598,21 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     BN_LAUNCH(k_bwd_fill, g, 256, 0, s, U.ia.p, U.ja.p, usrc.p, border.p, n, bia.p, bja.p, bsrc.p);
   }
   refresh_values();
+  remap(nullptr, s);
+}
+
+void IChol::remap(const int* inv, cudaStream_t s) {
+  const int m = offd_nnz > 0 ? offd_nnz : 1;
+  vorder.alloc(n, s);
+  vborder.alloc(n, s);
+  vfja.alloc(m, s);
+  vbja.alloc(m, s);
+  BN_LAUNCH(k_map_ids, grid_for(n, 256), 256, 0, s, order.p, n, inv, vorder.p);
+  BN_LAUNCH(k_map_ids, grid_for(n, 256), 256, 0, s, border.p, n, inv, vborder.p);
+  if (offd_nnz > 0) {
+    BN_LAUNCH(k_map_ids, grid_for(offd_nnz, 256), 256, 0, s, fja.p, offd_nnz, inv, vfja.p);
+    BN_LAUNCH(k_map_ids, grid_for(offd_nnz, 256), 256, 0, s, bja.p, offd_nnz, inv, vbja.p);
+  }
 }
 
 void IChol::refresh_values() {
@@ -501,6 +662,32 @@ static void run_tri(const std::vector<IChol::Seg>& segs, const int* ia, const in
 }
 
 template <class T>
+static void run_tri_coop(int nseg, const int4* segs, const int* ia, const int* ja, const T* val,
+                         const T* diag, const int* rows, const int* lptr, const T* in, T* x,
+                         cudaStream_t s) {
+  int dev = 0, per_sm = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_coop<T>, kCoopThreads, 0));
+  int sms = 0;
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int grid = sms * (per_sm < 4 ? per_sm : 4);
+  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): cooperative grid does not fit");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kCoopThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_coop<T>, ia, ja, val, diag, rows, lptr, segs, nseg, in,
+                             x));
+}
+
+template <class T>
 void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   const T* fv;
   const T* fd;
@@ -511,8 +698,13 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   } else {
     fv = fval32.p; fd = fdiag32.p; bv = bval32.p; bd = bdiag32.p;
   }
-  run_tri<T>(fseg, fia.p, fja.p, fv, fd, order.p, d_lptr.p, b, y, s);
-  run_tri<T>(bseg, bia.p, bja.p, bv, bd, border.p, d_bptr.p, y, x, s);
+  if (coop) {
+    run_tri_coop<T>(n_cfseg, d_cfseg.p, fia.p, vfja.p, fv, fd, vorder.p, d_lptr.p, b, y, s);
+    run_tri_coop<T>(n_cbseg, d_cbseg.p, bia.p, vbja.p, bv, bd, vborder.p, d_bptr.p, y, x, s);
+    return;
+  }
+  run_tri<T>(fseg, fia.p, vfja.p, fv, fd, vorder.p, d_lptr.p, b, y, s);
+  run_tri<T>(bseg, bia.p, vbja.p, bv, bd, vborder.p, d_bptr.p, y, x, s);
 }
 
 template void IChol::solve<double>(const double*, double*, double*, cudaStream_t);

@@ -23,8 +23,14 @@ struct IChol {
   std::vector<int> lptr, bptr;        // level offsets (forward / backward order)
   DBuf<int> d_lptr, d_bptr;
   std::vector<Seg> fseg, bseg;
+  DBuf<int4> d_cfseg, d_cbseg;  // cooperative schedules (narrow = 1024 rows)
+  int n_cfseg = 0, n_cbseg = 0;
+  bool coop = true;             // one cooperative launch per sweep
   DBuf<int> fia, fja, fsrc; // forward rows (level order)
   DBuf<int> bia, bja, bsrc; // backward rows (reverse level order)
+  // vector indices used by the solves: the rows/columns above mapped into
+  // the numbering of the vectors (the solve phase's colour-ordered one)
+  DBuf<int> vorder, vborder, vfja, vbja;
   DBuf<double> fval, bval, fdiag, bdiag;
   DBuf<float> fval32, bval32, fdiag32, bdiag32;
 
@@ -32,6 +38,7 @@ struct IChol {
   void load(CSR&& Lf, cudaStream_t s);          // take a factor as given (solve only)
   void finish(const int* aia, const int* aja, const double* aval, bool numeric, cudaStream_t s);
   void refresh_values();                        // (re)gather solve values from L
+  void remap(const int* inv, cudaStream_t s);   // vector numbering: inv[natural] (null: same)
   // x = (L L^T)^{-1} b ; y is scratch (n)
   template <class T>
   void solve(const T* b, T* y, T* x, cudaStream_t s);

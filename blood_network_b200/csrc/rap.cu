@@ -466,16 +466,24 @@ __global__ void k_iota64(long long* __restrict__ a, long long T) {
 
 // one thread per column segment: ordered sum; key for reordering = first
 // stream position of the column
+__global__ void k_gather_sorted(const long long* __restrict__ idx, long long T,
+                                const double* __restrict__ vals, double* __restrict__ out) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < T;
+       p += (long long)gridDim.x * blockDim.x)
+    out[p] = vals[idx[p]];
+}
+
+// svals: the products in sorted order (contiguous per column, stream order)
 __global__ void k_seg_sum(const unsigned long long* __restrict__ keys,
-                          const long long* __restrict__ idx, const double* __restrict__ vals,
+                          const long long* __restrict__ idx, const double* __restrict__ svals,
                           const long long* __restrict__ seg, long long nseg, long long T,
                           double* __restrict__ sval, int* __restrict__ scol,
                           long long* __restrict__ sfirst) {
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
        g += (long long)gridDim.x * blockDim.x) {
     const long long b = seg[g], e = (g + 1 < nseg) ? seg[g + 1] : T;
-    double v = vals[idx[b]];
-    for (long long p = b + 1; p < e; p++) v = xadd(v, vals[idx[p]]);
+    double v = svals[b];
+    for (long long p = b + 1; p < e; p++) v = xadd(v, svals[p]);
     sval[g] = v;
     scol[g] = (int)(keys[b] & 0xffffffffull);
     sfirst[g] = idx[b];
@@ -598,7 +606,9 @@ static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
   DBuf<int> scol(nseg, s);
   DBuf<long long> sfirst(nseg, s), sfirst2(nseg, s), g_in(nseg, s), g_out(nseg, s);
   DBuf<unsigned long long> srow(nseg, s);
-  BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, H.keys2.p, H.idx2.p, H.vals.p, H.seg.p,
+  DBuf<double> svals(T, s);
+  BN_LAUNCH(k_gather_sorted, grid_for(T, 256), 256, 0, s, H.idx2.p, T, H.vals.p, svals.p);
+  BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, H.keys2.p, H.idx2.p, svals.p, H.seg.p,
             nseg, T, sval.p, scol.p, sfirst.p);
   BN_LAUNCH(k_seg_rowkeys, grid_for(nseg, 256), 256, 0, s, H.keys2.p, H.seg.p, nseg, srow.p);
   BN_LAUNCH(k_iota64, grid_for(nseg, 256), 256, 0, s, g_in.p, nseg);

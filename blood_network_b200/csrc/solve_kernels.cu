@@ -223,15 +223,18 @@ int spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_
 // new values go to out[t] (Jacobi-style overflow classes whose rows may be
 // adjacent are computed into a buffer first, then scattered).
 template <class T, int G>
-__global__ void k_gs_color(const int* __restrict__ ia, const int* __restrict__ ja,
-                           const T* __restrict__ a, const int* __restrict__ rows, int nr,
-                           const T* __restrict__ b, T* x, T* __restrict__ out) {
+__device__ __forceinline__ void gs_rows_short(const int* __restrict__ ia,
+                                              const int* __restrict__ ja,
+                                              const T* __restrict__ a,
+                                              const int* __restrict__ rows, int r0, int nr,
+                                              const T* __restrict__ b, T* x, T* __restrict__ out,
+                                              int nblocks) {
   const int gl = threadIdx.x & (G - 1);
-  const int groups = (gridDim.x * blockDim.x) / G;
+  const int groups = (nblocks * blockDim.x) / G;
   unsigned gmask = 0xffffffffu;
   if constexpr (G < 32) gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) / G; t < nr; t += groups) {
-    const int i = rows[t];
+    const int i = rows ? rows[t] : r0 + t;
     T sum = T(0), d = T(0);
     bool has_d = false;
     for (int k = ia[i] + gl; k < ia[i + 1]; k += G) {
@@ -256,20 +259,19 @@ __global__ void k_gs_color(const int* __restrict__ ia, const int* __restrict__ j
   }
 }
 
-// one block per long row of a colour class
+// one block per long row
 template <class T>
-__global__ void __launch_bounds__(kLongThreads)
-k_gs_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
-          const int* __restrict__ rows, const T* __restrict__ b, T* x, T* __restrict__ out) {
+__device__ __forceinline__ void gs_row_long(const int* __restrict__ ia,
+                                            const int* __restrict__ ja, const T* __restrict__ a,
+                                            int t, int i, const T* __restrict__ b, T* x,
+                                            T* __restrict__ out) {
   __shared__ T red[kLongThreads / 32];
   __shared__ T dsh;
   __shared__ int has;
-  const int t = blockIdx.x;
-  const int i = rows[t];
   if (threadIdx.x == 0) { has = 0; dsh = T(1); }
   __syncthreads();
   T sum = T(0);
-  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += kLongThreads) {
+  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += blockDim.x) {
     const int j = ja[k];
     if (j == i) { dsh = a[k]; has = 1; }
     else sum = dadd(sum, dmul(a[k], x[j]));
@@ -285,47 +287,131 @@ k_gs_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __res
   }
 }
 
+// x_i = (b_i - sum_{j != i} a_ij x_j) / a_ii for the rows of one colour class
+// (cf_fwd_gs / cf_bwd_gs, C_amg1/src/amg_cycle.c:52-80; diagonal 1.0 if
+// missing).  Rows of a class share no edge, so a class is one launch: the
+// first nb_short blocks take the short rows (G lanes per row: 1 for the
+// short rows of fine levels, 8 or 32 for the denser coarse operators); each
+// further block takes one of the class's long rows (stored last).  With out
+// != nullptr the new values go to out[t] instead (an overflow class, whose
+// rows may be adjacent, is computed into a buffer first, then scattered).
+template <class T, int G>
+__global__ void __launch_bounds__(kLongThreads)
+k_gs_class(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+           const int* __restrict__ rows, int r0, int nshort, int nb_short,
+           const T* __restrict__ b, T* x, T* __restrict__ out) {
+  if ((int)blockIdx.x < nb_short) {
+    gs_rows_short<T, G>(ia, ja, a, rows, r0, nshort, b, x, out, nb_short);
+  } else {
+    const int t = nshort + (blockIdx.x - nb_short);
+    gs_row_long<T>(ia, ja, a, t, rows ? rows[t] : r0 + t, b, x, out);
+  }
+}
+
 template <class T>
-__global__ void k_scatter(const int* __restrict__ rows, int nr, const T* __restrict__ v,
+__global__ void k_scatter(const int* __restrict__ rows, int r0, int nr, const T* __restrict__ v,
                           T* __restrict__ x) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x)
-    x[rows[t]] = v[t];
+    x[rows ? rows[t] : r0 + t] = v[t];
 }
 
 template <class T>
-static void gs_launch(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* out,
-                      int group, cudaStream_t s, int nlong = 0) {
-  // the last nlong rows of the class are long rows: one block each
-  if (nlong > 0) {
-    BN_LAUNCH(k_gs_long<T>, nlong, kLongThreads, 0, s, A.ia, A.ja, A.val, rows + (nr - nlong), b,
-              x, out ? out + (nr - nlong) : nullptr);
-    nr -= nlong;
-    if (nr == 0) return;
-  }
+static void gs_launch(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x,
+                      T* out, int group, cudaStream_t s, int nlong = 0) {
+  const int nshort = nr - nlong;
+  int nb = 0;
+  if (nshort > 0)
+    nb = group >= 32 ? grid_for((long long)nshort * 32, kLongThreads, 8)
+                     : (group >= 8 ? grid_for((long long)nshort * 8, kLongThreads, 8)
+                                   : grid_for(nshort, kLongThreads, 8));
+  const int grid = nb + nlong;
+  if (grid == 0) return;
   if (group >= 32)
-    BN_LAUNCH((k_gs_color<T, 32>), grid_for((long long)nr * 32, 256, 8), 256, 0, s, A.ia, A.ja,
-              A.val, rows, nr, b, x, out);
+    BN_LAUNCH((k_gs_class<T, 32>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+              nb, b, x, out);
   else if (group >= 8)
-    BN_LAUNCH((k_gs_color<T, 8>), grid_for((long long)nr * 8, 256, 8), 256, 0, s, A.ia, A.ja,
-              A.val, rows, nr, b, x, out);
+    BN_LAUNCH((k_gs_class<T, 8>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+              nb, b, x, out);
   else
-    BN_LAUNCH((k_gs_color<T, 1>), grid_for(nr, 128, 16), 128, 0, s, A.ia, A.ja, A.val, rows, nr,
-              b, x, out);
+    BN_LAUNCH((k_gs_class<T, 1>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+              nb, b, x, out);
 }
 
 template <class T>
-void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
+void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, int group,
               cudaStream_t s, int nlong) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, nr, b, x, nullptr, group, s, nlong);
+  gs_launch<T>(A, rows, r0, nr, b, x, nullptr, group, s, nlong);
 }
 
 template <class T>
-void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
+void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, T* tmp,
                   int group, cudaStream_t s, int nlong) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, nr, b, x, tmp, group, s, nlong);
-  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, nr, tmp, x);
+  gs_launch<T>(A, rows, r0, nr, b, x, tmp, group, s, nlong);
+  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, r0, nr, tmp, x);
+}
+
+// A whole sweep of a small level in one 1024-thread block: classes in
+// order (or reverse), a barrier between classes; overflow classes are
+// computed into tmp and copied back.  Warp per row.
+template <class T>
+__global__ void __launch_bounds__(1024)
+k_gs_level_block(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+                 const int* __restrict__ cptr, const int* __restrict__ cjac, int ncls, int forward,
+                 const T* __restrict__ b, T* x, T* tmp) {
+  for (int q = 0; q < ncls; q++) {
+    const int c = forward ? q : ncls - 1 - q;
+    const int r0 = cptr[c], r1 = cptr[c + 1];
+    const bool jac = cjac[c] != 0;
+    const int lane = threadIdx.x & 31;
+    for (int i = r0 + (threadIdx.x >> 5); i < r1; i += (blockDim.x >> 5)) {
+      T sum = T(0), d = T(0);
+      int has = 0;
+      for (int k = ia[i] + lane; k < ia[i + 1]; k += 32) {
+        const int j = ja[k];
+        if (j == i) { d = a[k]; has = 1; }
+        else sum = dadd(sum, dmul(a[k], x[j]));
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        sum = dadd(sum, __shfl_xor_sync(0xffffffffu, sum, off));
+        const T od = __shfl_xor_sync(0xffffffffu, d, off);
+        const int oh = __shfl_xor_sync(0xffffffffu, has, off);
+        if (oh) { d = od; has = 1; }
+      }
+      if (lane == 0) {
+        const T xi = dsub(b[i], sum) / (has ? d : T(1));
+        if (jac) tmp[i - r0] = xi; else x[i] = xi;
+      }
+    }
+    __syncthreads();
+    if (jac) {
+      for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) x[i] = tmp[i - r0];
+      __syncthreads();
+    }
+  }
+}
+
+template <class T>
+void gs_level_block(const DevMat<T>& A, const int* cptr, const int* cjac, int ncls, bool forward,
+                    const T* b, T* x, T* tmp, cudaStream_t s) {
+  if (ncls <= 0) return;
+  BN_LAUNCH(k_gs_level_block<T>, 1, 1024, 0, s, A.ia, A.ja, A.val, cptr, cjac, ncls,
+            forward ? 1 : 0, b, x, tmp);
+}
+
+// out[t] = in[map[t]]  (gather) ; out[map[t]] = in[t]  (scatter)
+template <class T>
+__global__ void k_permute(const T* __restrict__ in, const int* __restrict__ map, int n,
+                          T* __restrict__ out, int scatter) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    if (scatter) out[map[t]] = in[t];
+    else out[t] = in[map[t]];
+  }
+}
+template <class T>
+void vpermute(const T* in, const int* map, int n, T* out, bool scatter, cudaStream_t s) {
+  if (n) BN_LAUNCH(k_permute<T>, grid_for(n, 256), 256, 0, s, in, map, n, out, scatter ? 1 : 0);
 }
 
 // ------------------------------------------------------------ vector ops
@@ -462,10 +548,13 @@ void pcg_scalars(double* sc, int flexible, cudaStream_t s) {
 #define BN_INST(T)                                                                           \
   template int spmv<T>(int, const DevMat<T>&, const T*, const T*, T*, cudaStream_t, const T*,  \
                        double*);                                                             \
-  template void gs_color<T>(const DevMat<T>&, const int*, int, const T*, T*, int,            \
+  template void gs_color<T>(const DevMat<T>&, const int*, int, int, const T*, T*, int,       \
                             cudaStream_t, int);                                              \
-  template void jacobi_class<T>(const DevMat<T>&, const int*, int, const T*, T*, T*, int,     \
+  template void jacobi_class<T>(const DevMat<T>&, const int*, int, int, const T*, T*, T*, int,\
                                 cudaStream_t, int);                                          \
+  template void vpermute<T>(const T*, const int*, int, T*, bool, cudaStream_t);              \
+  template void gs_level_block<T>(const DevMat<T>&, const int*, const int*, int, bool,       \
+                                  const T*, T*, T*, cudaStream_t);                           \
   template void vzero<T>(T*, int, cudaStream_t);                                             \
   template void vadd<T>(const T*, const T*, int, T*, cudaStream_t);                          \
   template void dot_partials<T>(const T*, const T*, const T*, int, double*, double*,          \

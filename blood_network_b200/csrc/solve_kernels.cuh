@@ -62,13 +62,21 @@ template <class T>
 int spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
          const T* dot_w = nullptr, double* partial = nullptr);
 int spmv_partials(int n, int nlong);
-// rows of one colour class; its last nlong rows are long rows (block each)
+// Rows of one colour class: rows[t] (or r0 + t when rows is null, a
+// contiguous class); its last nlong rows are long rows (one block each).
 template <class T>
-void gs_color(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, int group,
+void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, int group,
               cudaStream_t s, int nlong = 0);
 template <class T>
-void jacobi_class(const DevMat<T>& A, const int* rows, int nr, const T* b, T* x, T* tmp,
+void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, T* tmp,
                   int group, cudaStream_t s, int nlong = 0);
+// all colour classes of a small level, one block, one launch
+template <class T>
+void gs_level_block(const DevMat<T>& A, const int* cptr, const int* cjac, int ncls, bool forward,
+                    const T* b, T* x, T* tmp, cudaStream_t s);
+// gather out[t] = in[map[t]] or scatter out[map[t]] = in[t]
+template <class T>
+void vpermute(const T* in, const int* map, int n, T* out, bool scatter, cudaStream_t s);
 template <class T>
 void vzero(T* x, int n, cudaStream_t s);
 template <class TO, class TI>

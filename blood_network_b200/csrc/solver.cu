@@ -41,10 +41,12 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
 // of them taken joins the set's overflow class (colour kMaxColors), which the
 // smoother updates Jacobi-style.
 constexpr int kMaxColors = 32;
+constexpr int kCoarseColors = 8;
+constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
                               const int* __restrict__ set, int n, const int* __restrict__ color,
-                              int* __restrict__ newc, int* counter) {
+                              int* __restrict__ newc, int* counter, int cap) {
   int local = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     newc[i] = -1;
@@ -68,7 +70,8 @@ __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict_
       }
     }
     if (is_max) {
-      newc[i] = (used == 0xffffffffu) ? kMaxColors : __ffs(~used) - 1;
+      const int c = (used == 0xffffffffu) ? kMaxColors : __ffs(~used) - 1;
+      newc[i] = c < cap ? c : kMaxColors;
       local++;
     }
   }
@@ -132,11 +135,18 @@ __global__ void k_to_f32(const double* __restrict__ a, size_t m, T* __restrict__
 
 // ------------------------------------------------------------ data
 struct Level {
+  // setup data in the natural numbering (bit-identical to the reference)
   CSR A, S, P, R;
-  RowLayout layA, layP, layR;  // SpMV row-length layouts
   DBuf<int> cf;
   int n_coarse = 0;
   int max_lam = 0;
+  // solve phase: the level's unknowns renumbered so that every colour class
+  // is a contiguous range (perm[new] = natural, inv[natural] = new).  Ap is
+  // A renumbered on both sides; Pp maps the next level's numbering into this
+  // one; Rp = Pp^T.  FP32 value copies serve the mixed-precision V-cycle.
+  DBuf<int> perm, inv;
+  CSR Ap, Pp, Rp;
+  RowLayout layA, layP, layR;  // SpMV row-length layouts of Ap, Pp, Rp
   DBuf<float> A32, P32, R32;
   // smoother colouring: rows grouped by (set, colour)
   DBuf<int> gs_rows;
@@ -146,6 +156,7 @@ struct Level {
   int colored_for = -1;    // smoother the colouring was built for
   int color_rounds = 0;
   int gs_group = 1;        // lanes per row in the GS kernel
+  DBuf<int> d_cptr, d_cjac;  // class tables on the device (single-block sweeps)
   DBuf<double> l1, dg;
   DBuf<float> l1_32, dg32;
   // work vectors
@@ -160,6 +171,7 @@ struct Solver {
   std::vector<std::unique_ptr<Level>> lv;
   DenseCoarse coarse;
   CSR Aown;               // solve matrix when set_matrix replaced it
+  CSR Aownp;              // ... renumbered like level 0
   RowLayout layOwn;
   bool own_solve = false;
   DBuf<float> Aown32;
@@ -190,6 +202,8 @@ struct Solver {
   template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32,
                                    const RowLayout* lay) const;
   const RowLayout& lay_solve() const { return own_solve ? layOwn : lv[0]->layA; }
+  const CSR& Asolve_p() const { return own_solve ? Aownp : lv[0]->Ap; }
+  void build_solve_layout();
   template <class T> void smooth(int l, const T* bb, T* xl, bool forward);
   template <class T> void backslash(int l, const T* bb, T* xl);
   template <class T> void fwdslash(int l, const T* bb, T* xl);
@@ -230,12 +244,17 @@ void Solver::color_level(Level& L, int smoother) {
     set.alloc(n, s);
     BN_LAUNCH(k_cf_set, g, 256, 0, s, L.cf.p, n, set.p);
   }
+  // dense coarse operators get fewer colour classes (rows beyond the cap
+  // join the Jacobi-updated overflow class): each class costs a sequential
+  // step per sweep
+  const double avg_row = n > 0 ? (double)L.A.nnz / n : 0.0;
+  const int cap = avg_row > 16.0 ? kCoarseColors : kMaxColors;
   int done = 0, round = 0;
   while (done < n) {
     BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
     ctr.zero();
     BN_LAUNCH(k_color_round, g, 256, 0, s, L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, n,
-              color.p, newc.p, ctr.p);
+              color.p, newc.p, ctr.p, cap);
     BN_LAUNCH(k_color_commit, g, 256, 0, s, n, newc.p, color.p);
     done += read_scalar(ctr.p, s);
     round++;
@@ -269,8 +288,123 @@ void Solver::color_level(Level& L, int smoother) {
   }
   L.colored_for = smoother;
   L.color_rounds = round;
+  if (trace_on()) {
+    int ov = 0;
+    for (size_t c = 0; c + 1 < L.cptr.size(); c++)
+      if (L.cjac[c]) ov += L.cptr[c + 1] - L.cptr[c];
+    fprintf(stderr, "[bn]     colouring n=%d classes=%d overflow_rows=%d rounds=%d cap=%d\n", n,
+            (int)L.cptr.size() - 1, ov, round, cap);
+  }
+  {
+    const int nc = (int)L.cptr.size() - 1;
+    std::vector<int> jac(nc);
+    for (int c = 0; c < nc; c++) jac[c] = L.cjac[c];
+    L.d_cptr.alloc(nc + 1, s);
+    L.d_cptr.upload(L.cptr.data(), nc + 1);
+    L.d_cjac.alloc(nc > 0 ? nc : 1, s);
+    if (nc) L.d_cjac.upload(jac.data(), nc);
+    BN_CUDA(cudaStreamSynchronize(s));
+  }
   const double avg = n > 0 ? (double)L.A.nnz / n : 0.0;
   L.gs_group = avg <= 12.0 ? 1 : (avg <= 48.0 ? 8 : 32);
+}
+
+// B = rows perm[new] of A with columns renumbered by cinv (null: unchanged)
+__global__ void k_perm_count(const int* __restrict__ ia, const int* __restrict__ perm, int n,
+                             int* __restrict__ cnt) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const int o = perm ? perm[r] : r;
+    cnt[r] = ia[o + 1] - ia[o];
+  }
+}
+__global__ void k_perm_fill(const int* __restrict__ ia, const int* __restrict__ ja,
+                            const double* __restrict__ val, const int* __restrict__ perm,
+                            const int* __restrict__ cinv, int n, const int* __restrict__ bia,
+                            int* __restrict__ bja, double* __restrict__ bval) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+    const int o = perm ? perm[r] : r;
+    const int k0 = ia[o], len = ia[o + 1] - k0, q0 = bia[r];
+    for (int q = lane; q < len; q += 32) {
+      const int c = ja[k0 + q];
+      bja[q0 + q] = cinv ? cinv[c] : c;
+      bval[q0 + q] = val[k0 + q];
+    }
+  }
+}
+__global__ void k_inverse_perm(const int* __restrict__ perm, int n, int* __restrict__ inv) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    inv[perm[r]] = r;
+}
+__global__ void k_iota_perm(int* __restrict__ a, int n) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) a[r] = r;
+}
+
+static void permute_csr(const CSR& A, const int* perm, const int* cinv, CSR& B, cudaStream_t s) {
+  const int n = A.n;
+  DBuf<int> cnt((size_t)n + 1, s);
+  cnt.zero();
+  if (n > 0) BN_LAUNCH(k_perm_count, grid_for(n, 256), 256, 0, s, A.ia.p, perm, n, cnt.p);
+  const int nnz = scan_counts(cnt.p, n, s);
+  B.n = n;
+  B.m = A.m;
+  B.nnz = nnz;
+  B.ia = std::move(cnt);
+  B.ja.alloc((size_t)(nnz > 0 ? nnz : 1), s);
+  B.val.alloc((size_t)(nnz > 0 ? nnz : 1), s);
+  if (n > 0)
+    BN_LAUNCH(k_perm_fill, grid_for((long long)n * 32, 256), 256, 0, s, A.ia.p, A.ja.p, A.val.p,
+              perm, cinv, n, B.ia.p, B.ja.p, B.val.p);
+}
+
+// Colour-ordered renumbering of every level for the solve phase.
+void Solver::build_solve_layout() {
+  Phase ph("solve layout", s);
+  const int nl = (int)lv.size();
+  for (int l = 0; l < nl; l++) {
+    Level& L = *lv[l];
+    const int n = L.A.n;
+    L.perm.alloc(n > 0 ? n : 1, s);
+    L.inv.alloc(n > 0 ? n : 1, s);
+    const bool coloured = l < nl - 1 && L.gs_rows.n > 0 &&
+                          (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS);
+    if (n == 0) continue;
+    if (coloured)
+      BN_CUDA(cudaMemcpyAsync(L.perm.p, L.gs_rows.p, sizeof(int) * n, cudaMemcpyDeviceToDevice,
+                              s));
+    else
+      BN_LAUNCH(k_iota_perm, grid_for(n, 256), 256, 0, s, L.perm.p, n);
+    BN_LAUNCH(k_inverse_perm, grid_for(n, 256), 256, 0, s, L.perm.p, n, L.inv.p);
+  }
+  for (int l = 0; l < nl; l++) {
+    Level& L = *lv[l];
+    permute_csr(L.A, L.perm.p, L.inv.p, L.Ap, s);
+    analyze_rows(L.Ap, L.layA, s);
+    if (l < nl - 1) {
+      Level& C = *lv[l + 1];
+      permute_csr(L.P, L.perm.p, C.inv.p, L.Pp, s);
+      permute_csr(L.R, C.perm.p, L.inv.p, L.Rp, s);
+      analyze_rows(L.Pp, L.layP, s);
+      analyze_rows(L.Rp, L.layR, s);
+      if (opt.smoother == SMOOTHER_L1) {
+        L.l1.alloc(L.A.n, s);
+        BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.val.p, L.A.n,
+                  L.l1.p);
+      }
+      if (opt.smoother == SMOOTHER_JACOBI) {
+        L.dg.alloc(L.A.n, s);
+        BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.ja.p, L.Ap.val.p,
+                  L.A.n, L.dg.p);
+      }
+    }
+  }
+  if (own_solve) {
+    permute_csr(Aown, lv[0]->perm.p, lv[0]->inv.p, Aownp, s);
+    analyze_rows(Aownp, layOwn, s);
+  }
+  ic.remap(lv[0]->inv.p, s);
+  f32_ready = false;
 }
 
 void Solver::alloc_vectors() {
@@ -302,16 +436,16 @@ void Solver::prepare_f32() {
   const int nl = (int)lv.size();
   for (int l = 0; l < nl; l++) {
     Level& L = *lv[l];
-    L.A32.alloc(L.A.nnz > 0 ? L.A.nnz : 1, s);
-    BN_LAUNCH(k_to_f32<float>, grid_for(L.A.nnz, 256), 256, 0, s, L.A.val.p, (size_t)L.A.nnz,
+    L.A32.alloc(L.Ap.nnz > 0 ? L.Ap.nnz : 1, s);
+    BN_LAUNCH(k_to_f32<float>, grid_for(L.Ap.nnz, 256), 256, 0, s, L.Ap.val.p, (size_t)L.Ap.nnz,
               L.A32.p);
     if (l < nl - 1) {
-      L.P32.alloc(L.P.nnz > 0 ? L.P.nnz : 1, s);
-      L.R32.alloc(L.R.nnz > 0 ? L.R.nnz : 1, s);
-      BN_LAUNCH(k_to_f32<float>, grid_for(L.P.nnz, 256), 256, 0, s, L.P.val.p, (size_t)L.P.nnz,
-                L.P32.p);
-      BN_LAUNCH(k_to_f32<float>, grid_for(L.R.nnz, 256), 256, 0, s, L.R.val.p, (size_t)L.R.nnz,
-                L.R32.p);
+      L.P32.alloc(L.Pp.nnz > 0 ? L.Pp.nnz : 1, s);
+      L.R32.alloc(L.Rp.nnz > 0 ? L.Rp.nnz : 1, s);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.Pp.nnz, 256), 256, 0, s, L.Pp.val.p,
+                (size_t)L.Pp.nnz, L.P32.p);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.Rp.nnz, 256), 256, 0, s, L.Rp.val.p,
+                (size_t)L.Rp.nnz, L.R32.p);
       if (L.l1.n) {
         L.l1_32.alloc(L.l1.n, s);
         BN_LAUNCH(k_to_f32<float>, grid_for(L.l1.n, 256), 256, 0, s, L.l1.p, L.l1.n, L.l1_32.p);
@@ -323,9 +457,9 @@ void Solver::prepare_f32() {
     }
   }
   if (own_solve) {
-    Aown32.alloc(Aown.nnz > 0 ? Aown.nnz : 1, s);
-    BN_LAUNCH(k_to_f32<float>, grid_for(Aown.nnz, 256), 256, 0, s, Aown.val.p, (size_t)Aown.nnz,
-              Aown32.p);
+    Aown32.alloc(Aownp.nnz > 0 ? Aownp.nnz : 1, s);
+    BN_LAUNCH(k_to_f32<float>, grid_for(Aownp.nnz, 256), 256, 0, s, Aownp.val.p,
+              (size_t)Aownp.nnz, Aown32.p);
   }
   f32_ready = true;
 }
@@ -333,18 +467,6 @@ void Solver::prepare_f32() {
 void Solver::finish_setup() {
   const int nl = (int)lv.size();
   { Phase ph("dense coarse", s, nl - 1); coarse.setup(lv[nl - 1]->A, s); }
-  {
-    Phase ph("row layouts", s);
-    for (int l = 0; l < nl; l++) {
-      Level& L = *lv[l];
-      analyze_rows(L.A, L.layA, s);
-      if (l < nl - 1) {
-        analyze_rows(L.P, L.layP, s);
-        analyze_rows(L.R, L.layR, s);
-      }
-    }
-    if (own_solve) analyze_rows(Aown, layOwn, s);
-  }
   for (int l = 0; l < nl - 1; l++) {
     Level& L = *lv[l];
     const int sm = opt.smoother;
@@ -352,19 +474,10 @@ void Solver::finish_setup() {
       Phase ph("colouring", s, l);
       color_level(L, sm);
     }
-    if (sm == SMOOTHER_L1 && L.l1.n == 0) {
-      L.l1.alloc(L.A.n, s);
-      BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.A.ia.p, L.A.val.p, L.A.n, L.l1.p);
-    }
-    if (sm == SMOOTHER_JACOBI && L.dg.n == 0) {
-      L.dg.alloc(L.A.n, s);
-      BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.A.ia.p, L.A.ja.p, L.A.val.p, L.A.n,
-                L.dg.p);
-    }
   }
   ic.want_f32 = (opt.precision == AMG_PREC_MIXED);
   { Phase ph("ichol factor", s); ic.factor(Asolve(), s); }
-  f32_ready = false;
+  build_solve_layout();
   if (opt.precision == AMG_PREC_MIXED) { Phase ph("fp32 copies", s); prepare_f32(); }
   { Phase ph("vectors", s); alloc_vectors(); }
   drop_graphs();
@@ -419,11 +532,7 @@ void Solver::rebuild_values(CSR&& A0) {
     symmetrize(Ac, Acs, s);
     Level& nxt = *lv[k + 1];
     nxt.A = std::move(Acs);
-    nxt.l1.release();
-    nxt.dg.release();
   }
-  lv[0]->l1.release();
-  lv[0]->dg.release();
   own_solve = false;
   Aown = CSR();
   finish_setup();
@@ -439,7 +548,7 @@ template <class T>
 void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
   Level& L = *lv[l];
   const bool f64 = sizeof(T) == 8;
-  DevMat<T> A = mat<T>(L.A, &L.A32, &L.layA);
+  DevMat<T> A = mat<T>(L.Ap, &L.A32, &L.layA);
   const int n = L.A.n;
   for (int sweep = 0; sweep < opt.nu; sweep++) {
     switch (opt.smoother) {
@@ -447,14 +556,18 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
       case SMOOTHER_GS: {
         const int nseg = (int)L.cptr.size() - 1;
         T* tmp = f64 ? (T*)L.r.p : (T*)L.r32.p;
+        if (n <= kSmallLevel) {
+          gs_level_block<T>(A, L.d_cptr.p, L.d_cjac.p, nseg, forward, bb, xl, tmp, s);
+          break;
+        }
         for (int q = 0; q < nseg; q++) {
           int c = forward ? q : nseg - 1 - q;
-          const int* rows = L.gs_rows.p + L.cptr[c];
-          const int nr = L.cptr[c + 1] - L.cptr[c];
+          const int r0 = L.cptr[c];  // classes are contiguous in the solve numbering
+          const int nr = L.cptr[c + 1] - r0;
           if (L.cjac[c])
-            jacobi_class<T>(A, rows, nr, bb, xl, tmp, L.gs_group, s, L.clong[c]);
+            jacobi_class<T>(A, nullptr, r0, nr, bb, xl, tmp, L.gs_group, s, L.clong[c]);
           else
-            gs_color<T>(A, rows, nr, bb, xl, L.gs_group, s, L.clong[c]);
+            gs_color<T>(A, nullptr, r0, nr, bb, xl, L.gs_group, s, L.clong[c]);
         }
         break;
       }
@@ -491,11 +604,11 @@ void Solver::backslash(int l, const T* bb, T* xl) {
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
   { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
-  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.A, &L.A32, &L.layA), xl, bb, rr, s); }
-  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32, &L.layR), rr, nullptr, cb, s); }
+  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.Ap, &L.A32, &L.layA), xl, bb, rr, s); }
+  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), rr, nullptr, cb, s); }
   if (l + 1 < nl - 1) vzero<T>(cx, C.A.n, s);
   backslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_ADD, mat<T>(L.P, &L.P32, &L.layP), cx, nullptr, xl, s);  // x += P ec
+  spmv<T>(SPMV_ADD, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);  // x += P ec
 }
 
 // fwdslash_rec (amg_cycle.c:222-253); xl is zero on entry, so the first
@@ -512,9 +625,9 @@ void Solver::fwdslash(int l, const T* bb, T* xl) {
   const bool f64 = sizeof(T) == 8;
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
-  spmv<T>(SPMV_Y, mat<T>(L.R, &L.R32, &L.layR), bb, nullptr, cb, s);  // rc = P^T b
+  spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), bb, nullptr, cb, s);  // rc = P^T b
   fwdslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_Y, mat<T>(L.P, &L.P32, &L.layP), cx, nullptr, xl, s);  // x = P ec
+  spmv<T>(SPMV_Y, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);  // x = P ec
   smooth<T>(l, bb, xl, false);
 }
 
@@ -531,7 +644,7 @@ void Solver::precond_t(const T* g, T* out) {
   T* XX = f64 ? (T*)xx.p : (T*)xxf.p;
   T* R2 = f64 ? (T*)r2.p : (T*)r2f.p;
   T* CO = f64 ? (T*)corr.p : (T*)corrf.p;
-  DevMat<T> As = own_solve ? mat<T>(Aown, &Aown32, &layOwn) : mat<T>(lv[0]->A, &lv[0]->A32, &lv[0]->layA);
+  DevMat<T> As = own_solve ? mat<T>(Aownp, &Aown32, &layOwn) : mat<T>(lv[0]->Ap, &lv[0]->A32, &lv[0]->layA);
   vzero<T>(U1, n0, s);
   { Phase ph("backslash", s); backslash<T>(0, g, U1); }
   { Phase ph("residual r1", s); spmv<T>(SPMV_RES, As, U1, g, R1, s); }
@@ -590,10 +703,11 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   const int n0 = n();
   const bool flexible = (opt.precision == AMG_PREC_MIXED);
   if (flexible && !f32_ready) prepare_f32();
-  DevMat<double> A = mat<double>(Asolve(), nullptr, &lay_solve());
+  DevMat<double> A = mat<double>(Asolve_p(), nullptr, &lay_solve());
+  const int* perm0 = lv[0]->perm.p;
   cudaEventRecord(ev0, s);
-  BN_CUDA(cudaMemcpyAsync(b.p, d_b, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
-  BN_CUDA(cudaMemcpyAsync(x.p, d_x, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  vpermute<double>(d_b, perm0, n0, b.p, false, s);  // into the solve numbering
+  vpermute<double>(d_x, perm0, n0, x.p, false, s);
   spmv<double>(SPMV_RES, A, x.p, b.p, r.p, s);            // r = b - A x
   dot_partials<double>(b.p, b.p, r.p, n0, part0.p, part1.p, s);
   reduce_partials(part0.p, kRedBlocks, sc.p + SC_BB, s);  // b.b
@@ -654,7 +768,7 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   spmv<double>(SPMV_RES, A, x.p, b.p, ap.p, s);
   dot_partials<double>(ap.p, ap.p, nullptr, n0, part0.p, nullptr, s);
   reduce_partials(part0.p, kRedBlocks, sc.p + SC_RR, s);
-  BN_CUDA(cudaMemcpyAsync(d_x, x.p, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  vpermute<double>(x.p, perm0, n0, d_x, true, s);   // back to the caller's numbering
   cudaEventRecord(ev1, s);
   BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
   BN_CUDA(cudaStreamSynchronize(s));
@@ -720,6 +834,14 @@ static Solver* make_solver(int n, int nnz, const int* ia, const int* ja, const d
     S->opt.max_levels = AMG_MAX_LEVELS;
   S->device = o->device;
   BN_CUDA(cudaSetDevice(S->device));
+  {
+    // keep freed blocks in the stream-ordered pool instead of returning them
+    // at every synchronisation (setup synchronises often)
+    cudaMemPool_t pool;
+    BN_CUDA(cudaDeviceGetDefaultMemPool(&pool, S->device));
+    unsigned long long keep = ~0ull;
+    BN_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   BN_CUDA(cudaStreamCreateWithFlags(&S->s, cudaStreamNonBlocking));
   BN_CUDA(cudaEventCreate(&S->ev0));
   BN_CUDA(cudaEventCreate(&S->ev1));
@@ -823,9 +945,11 @@ BN_API int amg_solver_set_matrix(void* h, int n, int nnz, const int* ia, const i
     bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
     S->Aown = std::move(A);
     S->own_solve = true;
-    bn::analyze_rows(S->Aown, S->layOwn, S->s);
     S->ic.want_f32 = (S->opt.precision == AMG_PREC_MIXED);
     S->ic.factor(S->Aown, S->s);
+    bn::permute_csr(S->Aown, S->lv[0]->perm.p, S->lv[0]->inv.p, S->Aownp, S->s);
+    bn::analyze_rows(S->Aownp, S->layOwn, S->s);
+    S->ic.remap(S->lv[0]->inv.p, S->s);
     S->f32_ready = false;
     if (S->opt.precision == AMG_PREC_MIXED) S->prepare_f32();
     S->alloc_vectors();
@@ -847,18 +971,10 @@ BN_API void amg_solver_set_smoother(void* h, int smoother, double omega) {
       bn::Level& L = *S->lv[l];
       if ((smoother == SMOOTHER_CF_GS || smoother == SMOOTHER_GS) && L.colored_for != smoother)
         S->color_level(L, smoother);
-      if (smoother == SMOOTHER_L1 && L.l1.n == 0) {
-        L.l1.alloc(L.A.n, S->s);
-        BN_LAUNCH(bn::k_l1_diag, bn::grid_for(L.A.n, 256), 256, 0, S->s, L.A.ia.p, L.A.val.p,
-                  L.A.n, L.l1.p);
-      }
-      if (smoother == SMOOTHER_JACOBI && L.dg.n == 0) {
-        L.dg.alloc(L.A.n, S->s);
-        BN_LAUNCH(bn::k_diag, bn::grid_for(L.A.n, 256), 256, 0, S->s, L.A.ia.p, L.A.ja.p,
-                  L.A.val.p, L.A.n, L.dg.p);
-      }
     }
+    S->build_solve_layout();
     if (S->opt.precision == AMG_PREC_MIXED) S->prepare_f32();
+    S->alloc_vectors();
     S->drop_graphs();
     return 0;
   }, -1);
@@ -930,9 +1046,11 @@ BN_API int amg_solver_precond(void* h, const double* g, double* xo) {
     BN_CUDA(cudaSetDevice(S->device));
     const int n = S->n();
     if (S->opt.precision == AMG_PREC_MIXED && !S->f32_ready) S->prepare_f32();
-    bn::DBuf<double> dg(n, S->s), dx(n, S->s);
+    bn::DBuf<double> dg(n, S->s), dx(n, S->s), pg(n, S->s), px(n, S->s);
     dg.upload(g, n);
-    S->precond(dg.p, dx.p);
+    bn::vpermute<double>(dg.p, S->lv[0]->perm.p, n, pg.p, false, S->s);
+    S->precond(pg.p, px.p);
+    bn::vpermute<double>(px.p, S->lv[0]->perm.p, n, dx.p, true, S->s);
     dx.download(xo, n);
     BN_CUDA(cudaStreamSynchronize(S->s));
     int e = S->ic.take_error(S->s);
@@ -969,11 +1087,13 @@ BN_API int amg_solver_bench_kernel(void* h, int which, int precision, int reps, 
       switch (which) {
         case 0:
           if (f32)
-            bn::spmv<float>(bn::SPMV_RES, S->mat<float>(S->Asolve(), S->own_solve ? &S->Aown32 : &L0.A32,
+            bn::spmv<float>(bn::SPMV_RES, S->mat<float>(S->Asolve_p(),
+                                                         S->own_solve ? &S->Aown32 : &L0.A32,
                                                          &S->lay_solve()),
                             S->xxf.p, S->g32.p, S->r1f.p, S->s);
           else
-            bn::spmv<double>(bn::SPMV_RES, S->mat<double>(S->Asolve(), nullptr, &S->lay_solve()),
+            bn::spmv<double>(bn::SPMV_RES, S->mat<double>(S->Asolve_p(), nullptr,
+                                                          &S->lay_solve()),
                              S->x.p, S->b.p, S->r.p, S->s);
           break;
         case 1:
