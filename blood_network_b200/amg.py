@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ichol_compute": (None, [C.POINTER(DcsrMat), C.POINTER(IcholFactor)]),
         "ichol_solve": (None, [C.POINTER(IcholFactor), vp, vp]),
         "ichol_free": (None, [C.POINTER(IcholFactor)]),
+        "ichol_solve_noalloc": (i, [i, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -206,6 +206,26 @@ void ichol_compute(const dcsr_mat* A, ichol_factor* L);
 void ichol_solve(const ichol_factor* L, const double* b, double* x);
 void ichol_free(ichol_factor* L);
 
+/* ichol_solve_noalloc: no counterpart in the reference.  Solves L L^T x = b
+ * for an IC(0) factor already in device memory (0-based CSR d_ia[n+1],
+ * d_ja/d_val[nnz] as ichol_compute returns it, lower triangle, diagonal
+ * stored), with the same arithmetic as ichol_solve (bit-identical result),
+ * without allocating any memory: for callers that may not call cudaMalloc
+ * at the point where they apply the preconditioner (a memory budget owned by
+ * another framework, allocation-free callbacks).  Its scratch is a fixed
+ * device array of the library, so n <= AMG_NOALLOC_MAX_ROWS (larger n
+ * returns AMG_ERR_ARG with a message in amg_solver_last_error()).
+ * d_b and d_x are device pointers (n doubles each; they must not overlap);
+ * the launch is queued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) and the call returns without synchronising.  The first call on
+ * each device looks up that device's scratch address, so make it once before
+ * any stream capture.  All calls on a device share the scratch: calls that
+ * may overlap in time (other streams, other host threads) race -- order them
+ * on one stream.  Returns AMG_OK or a negative AMG_ERR_* code. */
+#define AMG_NOALLOC_MAX_ROWS 131072
+int ichol_solve_noalloc(int n, const int* d_ia, const int* d_ja, const double* d_val,
+                        const double* d_b, double* d_x, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
