@@ -17,11 +17,16 @@
 // Parallel schedule: row i depends on the rows k < i of its own pattern.
 // Dependency levels come from a Kahn frontier sweep (level l = rows whose
 // dependencies all lie in levels < l); rows are stored and processed in
-// level order.  Each level is one launch; runs of consecutive narrow levels
-// (tree parts, lattice corners) are batched into a single 1024-thread block
-// that steps through them with __syncthreads().  There are no cross-block
-// waits anywhere, so nothing can spin.
+// level order.  The factorization runs one launch per level; runs of
+// consecutive narrow levels (tree parts, lattice corners) are batched into a
+// single 1024-thread block that steps through them with __syncthreads().
+// The triangular solves run as one sync-free launch per sweep (rows wait on
+// their dependencies' values, every wait bounded), or, selectable, as level
+// launches or one cooperative launch with a grid barrier per level.
 #include "ichol.cuh"
+
+#include <cstdlib>
+#include <cstring>
 
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
@@ -348,6 +353,137 @@ k_tri_coop(const int* __restrict__ ia, const int* __restrict__ ja, const T* __re
   }
 }
 
+// Sync-free form: no barrier at all.  Every value of the output vector
+// starts as an all-ones bit pattern (a NaN that arithmetic never produces:
+// results are canonicalised below), so the value itself says whether it has
+// been computed.  A row polls each of its dependencies with relaxed GPU-scope
+// loads until the pattern is gone, then computes and publishes its value
+// with one relaxed store.  Rows are taken in level order, 32 per warp,
+// chunks dealt round-robin to the warps of a co-resident grid: a warp only
+// waits on rows of earlier chunks, and the earliest unfinished chunk has all
+// its dependencies done, so the sweep always advances.  Every wait is
+// bounded; a wait that runs out records an error and uses NaN, so the
+// kernel always ends and the failure surfaces as a non-finite result.
+template <class T>
+struct WordOf;
+template <>
+struct WordOf<float> {
+  using U = unsigned;
+  static constexpr U kPending = 0xFFFFFFFFu;
+  static constexpr U kNaN = 0x7FFFFFFFu;
+};
+template <>
+struct WordOf<double> {
+  using U = unsigned long long;
+  static constexpr U kPending = 0xFFFFFFFFFFFFFFFFull;
+  static constexpr U kNaN = 0x7FFFFFFFFFFFFFFFull;
+};
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ float word_value(unsigned u) { return __uint_as_float(u); }
+__device__ __forceinline__ double word_value(unsigned long long u) {
+  return __longlong_as_double((long long)u);
+}
+__device__ __forceinline__ unsigned value_word(float v) { return __float_as_uint(v); }
+__device__ __forceinline__ unsigned long long value_word(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+
+constexpr int kFlagThreads = 256;
+constexpr int kSpinFast = 64;          // polls before backing off
+constexpr int kSpinLimit = 1 << 22;    // polls before giving up (seconds with back-off)
+
+// Waits until none of the first m words u[q] (loaded from o[j[q]]) is
+// pending, re-polling all pending ones together so that the last arrival
+// costs one round trip.
+template <class U>
+__device__ __forceinline__ void wait_group(const U* o, const int (&j)[4], U (&u)[4], int m,
+                                           U pending, U nan, int* err) {
+  for (int it = 0; it < kSpinLimit; it++) {
+    bool pend = false;
+#pragma unroll
+    for (int q = 0; q < 4; q++) pend |= (q < m && u[q] == pending);
+    if (!pend) return;
+    if (it >= kSpinFast) __nanosleep(it < 4096 ? 32 : 256);
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < m && u[q] == pending) u[q] = ld_relaxed(o + j[q]);
+  }
+  atomicExch(err, 1);
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+    if (q < m && u[q] == pending) u[q] = nan;
+}
+
+// chunks[c] = [first, end) positions of chunk c: at most 32 rows, never
+// crossing a level boundary, so no lane waits on a lane of its own warp.
+// The warp reconverges after every chunk: lanes of one warp never spin on
+// different chunks at once.
+template <class T>
+__global__ void __launch_bounds__(kFlagThreads)
+k_tri_flags(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+            const T* __restrict__ diag, const int* __restrict__ rows,
+            const int2* __restrict__ chunks, int nchunks, const T* __restrict__ in, T* out,
+            T* clear, int* err) {
+  using W = WordOf<T>;
+  using U = typename W::U;
+  U* o = reinterpret_cast<U*>(out);
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int c = warp; c < nchunks; c += nwarps) {
+    const int2 ch = chunks[c];
+    const int t = ch.x + lane;
+    if (t < ch.y) {
+      const int i = rows[t];
+      const int k0 = ia[t], k1 = ia[t + 1];
+      T s = in[i];
+      const T d = diag[t];
+      if (clear) reinterpret_cast<U*>(clear)[i] = W::kPending;
+      for (int k = k0; k < k1; k += 4) {
+        const int m = k1 - k < 4 ? k1 - k : 4;
+        int j[4];
+        T v[4];
+        U u[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          j[q] = q < m ? ja[k + q] : 0;
+          v[q] = q < m ? val[k + q] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) u[q] = q < m ? ld_relaxed(o + j[q]) : U(0);
+        wait_group(o, j, u, m, W::kPending, W::kNaN, err);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (q < m) {
+            if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[q], word_value(u[q])));
+            else s = xsubf(s, xmulf(v[q], word_value(u[q])));
+          }
+        }
+      }
+      U r = value_word(s / d);
+      if (r == W::kPending) r = W::kNaN;
+      st_relaxed(o + i, r);
+    }
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------- layout
 __global__ void k_fwd_count(const int* __restrict__ lia, const int* __restrict__ lja,
                             const int* __restrict__ order, int n, int* __restrict__ cnt) {
@@ -437,6 +573,18 @@ static void make_segments(const std::vector<int>& ptr, std::vector<IChol::Seg>& 
       l = l1;
     }
   }
+}
+
+// 32-row chunks of the level-ordered layout, cut at every level boundary
+static int upload_chunks(const std::vector<int>& ptr, DBuf<int2>& d, cudaStream_t s) {
+  std::vector<int2> h;
+  for (size_t l = 0; l + 1 < ptr.size(); l++)
+    for (int t = ptr[l]; t < ptr[l + 1]; t += 32)
+      h.push_back(make_int2(t, t + 32 < ptr[l + 1] ? t + 32 : ptr[l + 1]));
+  d.alloc(h.size() > 0 ? h.size() : 1, s);
+  if (!h.empty()) d.upload(h.data(), h.size());
+  BN_CUDA(cudaStreamSynchronize(s));
+  return (int)h.size();
 }
 
 static void upload_segs(const std::vector<IChol::Seg>& segs, DBuf<int4>& d, cudaStream_t s) {
@@ -559,6 +707,8 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     n_cfseg = (int)cf.size();
     n_cbseg = (int)cb.size();
   }
+  n_fchunk = upload_chunks(lptr, d_fchunk, s);
+  n_bchunk = upload_chunks(bptr, d_bchunk, s);
   d_lptr.alloc(nlevels + 1, s);
   d_lptr.upload(lptr.data(), nlevels + 1);
   d_bptr.alloc(nlevels + 1, s);
@@ -599,6 +749,8 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   }
   refresh_values();
   remap(nullptr, s);
+  err.alloc(1, s);  // here, never inside a stream capture
+  err.zero();
 }
 
 void IChol::remap(const int* inv, cudaStream_t s) {
@@ -688,6 +840,32 @@ static void run_tri_coop(int nseg, const int4* segs, const int* ia, const int* j
 }
 
 template <class T>
+static void run_tri_flags(int nchunks, const int2* chunks, int blocks_per_sm, const int* ia,
+                          const int* ja, const T* val, const T* diag, const int* rows,
+                          const T* in, T* out, T* clear, int* err, cudaStream_t s) {
+  int dev = 0, per_sm = 0, sms = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_flags<T>, kFlagThreads, 0));
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (blocks_per_sm > 0 && per_sm > blocks_per_sm) per_sm = blocks_per_sm;
+  const int grid = sms * per_sm;
+  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): sweep grid does not fit");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kFlagThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_flags<T>, ia, ja, val, diag, rows, chunks, nchunks, in,
+                             out, clear, err));
+}
+
+template <class T>
 void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   const T* fv;
   const T* fd;
@@ -698,7 +876,16 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   } else {
     fv = fval32.p; fd = fdiag32.p; bv = bval32.p; bd = bdiag32.p;
   }
-  if (coop) {
+  if (mode == kSweepFlags) {
+    if (n == 0) return;
+    BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
+    run_tri_flags<T>(n_fchunk, d_fchunk.p, blocks_per_sm, fia.p, vfja.p, fv, fd, vorder.p, b, y,
+                     x, err.p, s);
+    run_tri_flags<T>(n_bchunk, d_bchunk.p, blocks_per_sm, bia.p, vbja.p, bv, bd, vborder.p, y, x,
+                     nullptr, err.p, s);
+    return;
+  }
+  if (mode == kSweepCoop) {
     run_tri_coop<T>(n_cfseg, d_cfseg.p, fia.p, vfja.p, fv, fd, vorder.p, d_lptr.p, b, y, s);
     run_tri_coop<T>(n_cbseg, d_cbseg.p, bia.p, vbja.p, bv, bd, vborder.p, d_bptr.p, y, x, s);
     return;
@@ -710,6 +897,24 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
 template void IChol::solve<double>(const double*, double*, double*, cudaStream_t);
 template void IChol::solve<float>(const float*, float*, float*, cudaStream_t);
 
-int IChol::take_error(cudaStream_t) { return 0; }
+int IChol::take_error(cudaStream_t s) {
+  if (!err.p) return 0;
+  int e = read_scalar(err.p, s);
+  if (e) err.zero();
+  return e ? BN_ERR_SPIN : 0;
+}
+
+int IChol::blocks_from_env() {
+  const char* v = getenv("BN_IC_BLOCKS");
+  return v ? atoi(v) : 2;  // 2 blocks of 256 per SM measured fastest on the 20M network
+}
+
+int IChol::mode_from_env() {
+  const char* v = getenv("BN_IC_MODE");
+  if (!v) return kSweepFlags;
+  if (!strcmp(v, "levels")) return kSweepLevels;
+  if (!strcmp(v, "coop")) return kSweepCoop;
+  return kSweepFlags;
+}
 
 }  // namespace bn

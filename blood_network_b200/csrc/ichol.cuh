@@ -25,7 +25,14 @@ struct IChol {
   std::vector<Seg> fseg, bseg;
   DBuf<int4> d_cfseg, d_cbseg;  // cooperative schedules (narrow = 1024 rows)
   int n_cfseg = 0, n_cbseg = 0;
-  bool coop = true;             // one cooperative launch per sweep
+  // sweep form: level launches, one cooperative launch with a grid barrier
+  // per level, or the sync-free form (default; BN_IC_MODE=levels|coop|flags)
+  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2 };
+  int mode = mode_from_env();
+  int blocks_per_sm = blocks_from_env();  // sync-free grid: blocks per SM (0: occupancy)
+  DBuf<int> err;                // sync-free form: a wait ran out
+  DBuf<int2> d_fchunk, d_bchunk;  // sync-free form: 32-row chunks within levels
+  int n_fchunk = 0, n_bchunk = 0;
   DBuf<int> fia, fja, fsrc; // forward rows (level order)
   DBuf<int> bia, bja, bsrc; // backward rows (reverse level order)
   // vector indices used by the solves: the rows/columns above mapped into
@@ -42,7 +49,9 @@ struct IChol {
   // x = (L L^T)^{-1} b ; y is scratch (n)
   template <class T>
   void solve(const T* b, T* y, T* x, cudaStream_t s);
-  int take_error(cudaStream_t s);               // no device waits remain: always 0
+  int take_error(cudaStream_t s);               // BN_ERR_SPIN if a wait ran out (then cleared)
+  static int mode_from_env();
+  static int blocks_from_env();
   int launches_per_solve() const { return (int)(fseg.size() + bseg.size()); }
 };
 
