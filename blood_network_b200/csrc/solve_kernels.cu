@@ -338,6 +338,14 @@ static void gs_launch(const DevMat<T>& A, const int* rows, int r0, int nr, const
 }
 
 template <class T>
+void scatter_range(const T* v, int r0, int nr, T* x, cudaStream_t s) {
+  if (nr == 0) return;
+  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, nullptr, r0, nr, v, x);
+}
+template void scatter_range<double>(const double*, int, int, double*, cudaStream_t);
+template void scatter_range<float>(const float*, int, int, float*, cudaStream_t);
+
+template <class T>
 void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, int group,
               cudaStream_t s, int nlong) {
   if (nr == 0) return;

@@ -70,6 +70,9 @@ void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T
 template <class T>
 void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, T* tmp,
                   int group, cudaStream_t s, int nlong = 0);
+// x[r0 + t] = v[t], t < nr
+template <class T>
+void scatter_range(const T* v, int r0, int nr, T* x, cudaStream_t s);
 // all colour classes of a small level, one block, one launch
 template <class T>
 void gs_level_block(const DevMat<T>& A, const int* cptr, const int* cjac, int ncls, bool forward,

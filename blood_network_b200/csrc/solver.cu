@@ -15,6 +15,7 @@
 #include "ichol.cuh"
 #include "dense.cuh"
 #include "solve_kernels.cuh"
+#include "packed.cuh"
 #include "../../include/amg_b200.h"
 
 #include <cub/cub.cuh>
@@ -159,6 +160,12 @@ struct Level {
   DBuf<int> d_cptr, d_cjac;  // class tables on the device (single-block sweeps)
   DBuf<double> l1, dg;
   DBuf<float> l1_32, dg32;
+  // load-balanced kernels: packings of Ap, Pp, Rp (one range each) and of
+  // the colour classes of Ap (one range per class)
+  Packing pkA, pkP, pkR, pkG;
+  // which operators run on the packed kernels: those with rows longer than
+  // kLongRow (hub rows); the row-group kernels are faster on the others
+  bool use_pkA = false, use_pkP = false, use_pkR = false;
   // work vectors
   DBuf<double> b, x, r;
   DBuf<float> b32, x32, r32;
@@ -201,6 +208,11 @@ struct Solver {
   void drop_graphs();
   template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32,
                                    const RowLayout* lay) const;
+  template <class T> PackedMat<T> pmat(const CSR& M, const DBuf<float>& v32,
+                                       const Packing& pk) const;
+  // V-cycle SpMV and colour classes on the packed kernels (BN_PACKED=0: the
+  // row-group kernels)
+  bool use_packed = getenv("BN_PACKED") == nullptr || atoi(getenv("BN_PACKED")) != 0;
   const RowLayout& lay_solve() const { return own_solve ? layOwn : lv[0]->layA; }
   const CSR& Asolve_p() const { return own_solve ? Aownp : lv[0]->Ap; }
   void build_solve_layout();
@@ -232,6 +244,24 @@ DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32, const RowLayout* lay
   else d.val = v32->p;
   if (lay) { d.group = lay->group; d.lrows = lay->lrows.p; d.nlong = lay->nlong; }
   return d;
+}
+
+template <class T>
+PackedMat<T> Solver::pmat(const CSR& M, const DBuf<float>& v32, const Packing& pk) const {
+  PackedMat<T> d;
+  d.ia = M.ia.p;
+  d.ja = M.ja.p;
+  if constexpr (sizeof(T) == 8) d.val = M.val.p;
+  else d.val = v32.p;
+  d.pk = &pk;
+  return d;
+}
+
+static std::vector<int> host_ia(const CSR& M, cudaStream_t s) {
+  std::vector<int> h((size_t)M.n + 1);
+  M.ia.download(h.data(), (size_t)M.n + 1);
+  BN_CUDA(cudaStreamSynchronize(s));
+  return h;
 }
 
 void Solver::color_level(Level& L, int smoother) {
@@ -362,13 +392,16 @@ static void permute_csr(const CSR& A, const int* perm, const int* cinv, CSR& B, 
 void Solver::build_solve_layout() {
   Phase ph("solve layout", s);
   const int nl = (int)lv.size();
+  auto coloured_level = [&](int l) {
+    return l < nl - 1 && lv[l]->gs_rows.n > 0 &&
+           (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS);
+  };
   for (int l = 0; l < nl; l++) {
     Level& L = *lv[l];
     const int n = L.A.n;
     L.perm.alloc(n > 0 ? n : 1, s);
     L.inv.alloc(n > 0 ? n : 1, s);
-    const bool coloured = l < nl - 1 && L.gs_rows.n > 0 &&
-                          (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS);
+    const bool coloured = coloured_level(l);
     if (n == 0) continue;
     if (coloured)
       BN_CUDA(cudaMemcpyAsync(L.perm.p, L.gs_rows.p, sizeof(int) * n, cudaMemcpyDeviceToDevice,
@@ -392,7 +425,27 @@ void Solver::build_solve_layout() {
         BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.val.p, L.A.n,
                   L.l1.p);
       }
-      if (opt.smoother == SMOOTHER_JACOBI) {
+      if (use_packed) {
+        Phase ph2("packing", s, l);
+        std::vector<int> ha = host_ia(L.Ap, s);
+        L.pkA.build(ha, {make_int2(0, L.Ap.n)}, s);
+        if (coloured_level(l)) {
+          std::vector<int2> rg;
+          for (size_t c = 0; c + 1 < L.cptr.size(); c++) rg.push_back(make_int2(L.cptr[c], L.cptr[c + 1]));
+          L.pkG.build(ha, rg, s);
+        }
+        std::vector<int> hp = host_ia(L.Pp, s);
+        L.pkP.build(hp, {make_int2(0, L.Pp.n)}, s);
+        std::vector<int> hr = host_ia(L.Rp, s);
+        L.pkR.build(hr, {make_int2(0, L.Rp.n)}, s);
+        L.use_pkA = L.layA.nlong > 0;
+        L.use_pkP = L.layP.nlong > 0;
+        L.use_pkR = L.layR.nlong > 0;
+        if (trace_on())
+          fprintf(stderr, "[bn] L%d packed kernels: A %d (%d long rows)  P %d  R %d (%d long rows)\n",
+                  l, (int)L.use_pkA, L.layA.nlong, (int)L.use_pkP, (int)L.use_pkR, L.layR.nlong);
+      }
+      if (opt.smoother == SMOOTHER_JACOBI || coloured_level(l)) {
         L.dg.alloc(L.A.n, s);
         BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.ja.p, L.Ap.val.p,
                   L.A.n, L.dg.p);
@@ -560,6 +613,22 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
           gs_level_block<T>(A, L.d_cptr.p, L.d_cjac.p, nseg, forward, bb, xl, tmp, s);
           break;
         }
+        if (use_packed && L.use_pkA && L.pkG.ranges() == nseg) {
+          const T* d = f64 ? (const T*)L.dg.p : (const T*)L.dg32.p;
+          PackedMat<T> G = pmat<T>(L.Ap, L.A32, L.pkG);
+          for (int q = 0; q < nseg; q++) {
+            const int c = forward ? q : nseg - 1 - q;
+            const int r0 = L.cptr[c];
+            const int nr = L.cptr[c + 1] - r0;
+            if (L.cjac[c]) {
+              packed_apply<T>(PK_JAC, G, c, xl, bb, tmp, d, r0, s);
+              scatter_range<T>(tmp, r0, nr, xl, s);
+            } else {
+              packed_apply<T>(PK_GS, G, c, xl, bb, xl, d, r0, s);
+            }
+          }
+          break;
+        }
         for (int q = 0; q < nseg; q++) {
           int c = forward ? q : nseg - 1 - q;
           const int r0 = L.cptr[c];  // classes are contiguous in the solve numbering
@@ -604,11 +673,26 @@ void Solver::backslash(int l, const T* bb, T* xl) {
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
   { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
-  { Phase ph("residual", s, l); spmv<T>(SPMV_RES, mat<T>(L.Ap, &L.A32, &L.layA), xl, bb, rr, s); }
-  { Phase ph("restrict", s, l); spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), rr, nullptr, cb, s); }
+  {
+    Phase ph("residual", s, l);
+    if (use_packed && L.use_pkA)
+      packed_apply<T>(PK_RES, pmat<T>(L.Ap, L.A32, L.pkA), 0, xl, bb, rr, nullptr, 0, s);
+    else
+      spmv<T>(SPMV_RES, mat<T>(L.Ap, &L.A32, &L.layA), xl, bb, rr, s);
+  }
+  {
+    Phase ph("restrict", s, l);
+    if (use_packed && L.use_pkR)
+      packed_apply<T>(PK_Y, pmat<T>(L.Rp, L.R32, L.pkR), 0, rr, nullptr, cb, nullptr, 0, s);
+    else
+      spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), rr, nullptr, cb, s);
+  }
   if (l + 1 < nl - 1) vzero<T>(cx, C.A.n, s);
   backslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_ADD, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);  // x += P ec
+  if (use_packed && L.use_pkP)  // x += P ec
+    packed_apply<T>(PK_ADD, pmat<T>(L.Pp, L.P32, L.pkP), 0, cx, nullptr, xl, nullptr, 0, s);
+  else
+    spmv<T>(SPMV_ADD, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);
 }
 
 // fwdslash_rec (amg_cycle.c:222-253); xl is zero on entry, so the first
@@ -625,9 +709,15 @@ void Solver::fwdslash(int l, const T* bb, T* xl) {
   const bool f64 = sizeof(T) == 8;
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
-  spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), bb, nullptr, cb, s);  // rc = P^T b
+  if (use_packed && L.use_pkR)  // rc = P^T b
+    packed_apply<T>(PK_Y, pmat<T>(L.Rp, L.R32, L.pkR), 0, bb, nullptr, cb, nullptr, 0, s);
+  else
+    spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), bb, nullptr, cb, s);
   fwdslash<T>(l + 1, cb, cx);
-  spmv<T>(SPMV_Y, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);  // x = P ec
+  if (use_packed && L.use_pkP)  // x = P ec
+    packed_apply<T>(PK_Y, pmat<T>(L.Pp, L.P32, L.pkP), 0, cx, nullptr, xl, nullptr, 0, s);
+  else
+    spmv<T>(SPMV_Y, mat<T>(L.Pp, &L.P32, &L.layP), cx, nullptr, xl, s);
   smooth<T>(l, bb, xl, false);
 }
 
@@ -647,10 +737,24 @@ void Solver::precond_t(const T* g, T* out) {
   DevMat<T> As = own_solve ? mat<T>(Aownp, &Aown32, &layOwn) : mat<T>(lv[0]->Ap, &lv[0]->A32, &lv[0]->layA);
   vzero<T>(U1, n0, s);
   { Phase ph("backslash", s); backslash<T>(0, g, U1); }
-  { Phase ph("residual r1", s); spmv<T>(SPMV_RES, As, U1, g, R1, s); }
+  const bool fine_packed = use_packed && !own_solve && lv[0]->use_pkA && lv[0]->pkA.ranges() == 1;
+  PackedMat<T> Ap0 = pmat<T>(lv[0]->Ap, lv[0]->A32, lv[0]->pkA);
+  if (fine_packed) {
+    Phase ph("residual r1", s);
+    packed_apply<T>(PK_RES, Ap0, 0, U1, g, R1, nullptr, 0, s);
+  } else {
+    Phase ph("residual r1", s);
+    spmv<T>(SPMV_RES, As, U1, g, R1, s);
+  }
   { Phase ph("ichol solve", s); ic.solve<T>(R1, IY, IX, s); }
   vadd<T>(U1, IX, n0, XX, s);
-  { Phase ph("residual r2", s); spmv<T>(SPMV_RES, As, XX, g, R2, s); }
+  if (fine_packed) {
+    Phase ph("residual r2", s);
+    packed_apply<T>(PK_RES, Ap0, 0, XX, g, R2, nullptr, 0, s);
+  } else {
+    Phase ph("residual r2", s);
+    spmv<T>(SPMV_RES, As, XX, g, R2, s);
+  }
   { Phase ph("fwdslash", s); fwdslash<T>(0, R2, CO); }
   vadd<T>(XX, CO, n0, out, s);
 }
