@@ -40,6 +40,7 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
     const int i = r0 + threadIdx.x;
     T hold = T(0);
     if (e1 - e0 <= kTileNnz) {
+#pragma unroll 4
       for (int k = e0 + threadIdx.x; k < e1; k += kRows) prod[k - e0] = dmul(a[k], x[ja[k]]);
       __syncthreads();
       if (i < r1) {
@@ -93,6 +94,7 @@ k_spmv_vec(const int* __restrict__ ia, const int* __restrict__ ja, const T* __re
     const int k0 = ia[i], k1 = ia[i + 1];
     if (skip_long && k1 - k0 > kLongRow) continue;  // long-row kernel
     T sum = T(0);
+#pragma unroll 4
     for (int k = k0 + gl; k < k1; k += G) sum = dadd(sum, dmul(a[k], x[ja[k]]));
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) sum = dadd(sum, __shfl_xor_sync(gmask, sum, off, G));
@@ -237,6 +239,7 @@ __device__ __forceinline__ void gs_rows_short(const int* __restrict__ ia,
     const int i = rows ? rows[t] : r0 + t;
     T sum = T(0), d = T(0);
     bool has_d = false;
+#pragma unroll 4
     for (int k = ia[i] + gl; k < ia[i + 1]; k += G) {
       const int j = ja[k];
       const T v = a[k];
