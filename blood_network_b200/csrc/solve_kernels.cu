@@ -26,43 +26,67 @@ template <> __device__ __forceinline__ double dsub(double a, double b) { return 
 template <> __device__ __forceinline__ float dsub(float a, float b) { return __fsub_rn(a, b); }
 
 // -------------------------------------------------------------------- SpMV
+// Each thread's tile header (the tile's nonzero range, its own row range,
+// its b_i / y_i and dot weight) is loaded one tile ahead, so those loads are
+// in flight while the current tile computes.
 template <class T, int MODE, bool DOT>
-__global__ void __launch_bounds__(kRows)
+__global__ void __launch_bounds__(kRows, 8)
 k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
        const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
-       const T* __restrict__ dw, double* __restrict__ partial, int skip_long) {
+       const T* __restrict__ dw, double* __restrict__ partial, int skip_long,
+       const int* __restrict__ tiles) {
   __shared__ T prod[kTileNnz];
   __shared__ double red[kRows / 32];
   double dot = 0.0;
-  for (int r0 = blockIdx.x * kRows; r0 < n; r0 += gridDim.x * kRows) {
+  const int ntiles = (n + kRows - 1) / kRows;
+  int e0 = 0, e1 = 0, k0 = 0, k1 = 0;
+  T hb = T(0), hw = T(0);
+  auto head = [&](int t0) {
+    const int t1 = min(t0 + kRows, n);
+    e0 = ia[t0];
+    e1 = ia[t1];
+    const int i = t0 + threadIdx.x;
+    if (i < t1) {
+      k0 = ia[i];
+      k1 = ia[i + 1];
+      if (MODE == SPMV_RES) hb = b[i];
+      if (MODE == SPMV_ADD) hb = y[i];
+      if (DOT) hw = dw[i];
+    }
+  };
+  auto tile_row = [&](int slot) { return (tiles ? tiles[slot] : slot) * kRows; };
+  int nxt = (int)blockIdx.x < ntiles ? tile_row(blockIdx.x) : 0;
+  if ((int)blockIdx.x < ntiles) head(nxt);
+  for (int slot = blockIdx.x; slot < ntiles; slot += gridDim.x) {
+    const int r0 = nxt;
     const int r1 = min(r0 + kRows, n);
-    const int e0 = ia[r0], e1 = ia[r1];
     const int i = r0 + threadIdx.x;
-    T hold = T(0);
-    if (e1 - e0 <= kTileNnz) {
+    const int ce0 = e0, ce1 = e1, ck0 = k0, ck1 = k1;
+    const T cb = hb, cw = hw;
+    if (slot + (int)gridDim.x < ntiles) {
+      nxt = tile_row(slot + gridDim.x);
+      head(nxt);
+    }
+    T hold = (MODE == SPMV_Y) ? T(0) : cb;
+    if (ce1 - ce0 <= kTileNnz) {
 #pragma unroll 4
-      for (int k = e0 + threadIdx.x; k < e1; k += kRows) prod[k - e0] = dmul(a[k], x[ja[k]]);
+      for (int k = ce0 + threadIdx.x; k < ce1; k += kRows) prod[k - ce0] = dmul(a[k], x[ja[k]]);
       __syncthreads();
       if (i < r1) {
-        if (MODE == SPMV_RES) hold = b[i];
-        if (MODE == SPMV_ADD) hold = y[i];
-        const int k0 = ia[i] - e0, k1 = ia[i + 1] - e0;
-        for (int k = k0; k < k1; k++)
+        for (int k = ck0 - ce0; k < ck1 - ce0; k++)
           hold = (MODE == SPMV_RES) ? dsub(hold, prod[k]) : dadd(hold, prod[k]);
       }
       __syncthreads();
     } else if (i < r1) {
-      if (skip_long && ia[i + 1] - ia[i] > kLongRow) continue;  // long-row kernel
-      if (MODE == SPMV_RES) hold = b[i];
-      if (MODE == SPMV_ADD) hold = y[i];
-      for (int k = ia[i]; k < ia[i + 1]; k++) {
+      if (skip_long && ck1 - ck0 > kLongRow) continue;  // long-row kernel
+      for (int k = ck0; k < ck1; k++) {
         T p = dmul(a[k], x[ja[k]]);
         hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
       }
     }
     if (i < r1) {
       y[i] = hold;
-      if (DOT) dot += (double)dw[i] * (double)hold;
+      if (DOT) dot += (double)cw * (double)hold;
     }
   }
   if (DOT) {
@@ -172,6 +196,29 @@ void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {
 
 int spmv_partials(int n, int nlong) { return spmv_grid(n) + nlong; }
 
+__global__ void k_tile_keys(const int* __restrict__ key, int n, int ntiles, int* __restrict__ tk,
+                            int* __restrict__ ids) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    tk[t] = key[t * kRows];
+    ids[t] = t;
+  }
+}
+
+void order_tiles(int n, const int* key, RowLayout& out, cudaStream_t s) {
+  const int ntiles = (n + kRows - 1) / kRows;
+  if (ntiles <= 1 || !key) { out.tiles = DBuf<int>(); return; }
+  DBuf<int> tk(ntiles, s), tk2(ntiles, s), ids(ntiles, s);
+  out.tiles.alloc(ntiles, s);
+  BN_LAUNCH(k_tile_keys, grid_for(ntiles, 256), 256, 0, s, key, n, ntiles, tk.p, ids.p);
+  size_t tmp = 0;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, tk.p, tk2.p, ids.p, out.tiles.p, ntiles, 0,
+                                          32, s));
+  DBuf<unsigned char> t(tmp, s);
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, tk.p, tk2.p, ids.p, out.tiles.p, ntiles, 0, 32,
+                                          s));
+  BN_CUDA(cudaStreamSynchronize(s));
+}
+
 template <class T, int MODE, bool DOT>
 static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
                           const T* dw, double* partial) {
@@ -180,7 +227,7 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
   switch (A.group) {
     case 0:
       BN_LAUNCH((k_spmv<T, MODE, DOT>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dw,
-                partial, skip);
+                partial, skip, A.tiles);
       break;
     case 4:
       BN_LAUNCH((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,

@@ -40,15 +40,21 @@ struct DevMat {
   int group = 0;
   const int* lrows = nullptr;
   int nlong = 0;
+  const int* tiles = nullptr;  // row-tile kernel: order in which tiles are visited (null: natural)
 };
 
 // Row-length layout of a CSR matrix (computed once at setup).
 struct RowLayout {
   int group = 0;
+  DBuf<int> tiles;  // visiting order of the kRows-row tiles (empty: natural)
   DBuf<int> lrows;
   int nlong = 0;
 };
 void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s);
+// Visit the row tiles of a matrix in the order of key[first row of tile]
+// (rows renumbered into colour classes: key = original row number, so that
+// concurrently processed tiles gather from one neighbourhood of x).
+void order_tiles(int n, const int* key, RowLayout& out, cudaStream_t s);
 
 inline int spmv_grid(int n) {
   int tiles = (n + kRows - 1) / kRows;

@@ -242,7 +242,12 @@ DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32, const RowLayout* lay
   d.n = M.n; d.m = M.m; d.nnz = M.nnz; d.ia = M.ia.p; d.ja = M.ja.p;
   if constexpr (sizeof(T) == 8) d.val = M.val.p;
   else d.val = v32->p;
-  if (lay) { d.group = lay->group; d.lrows = lay->lrows.p; d.nlong = lay->nlong; }
+  if (lay) {
+    d.group = lay->group;
+    d.lrows = lay->lrows.p;
+    d.nlong = lay->nlong;
+    d.tiles = lay->tiles.n ? lay->tiles.p : nullptr;
+  }
   return d;
 }
 
@@ -414,12 +419,16 @@ void Solver::build_solve_layout() {
     Level& L = *lv[l];
     permute_csr(L.A, L.perm.p, L.inv.p, L.Ap, s);
     analyze_rows(L.Ap, L.layA, s);
+    // row tiles in original row order: classes interleave, x gathers stay local
+    if (coloured_level(l)) order_tiles(L.Ap.n, L.perm.p, L.layA, s);
     if (l < nl - 1) {
       Level& C = *lv[l + 1];
       permute_csr(L.P, L.perm.p, C.inv.p, L.Pp, s);
       permute_csr(L.R, C.perm.p, L.inv.p, L.Rp, s);
       analyze_rows(L.Pp, L.layP, s);
       analyze_rows(L.Rp, L.layR, s);
+      if (coloured_level(l)) order_tiles(L.Pp.n, L.perm.p, L.layP, s);
+      if (coloured_level(l + 1)) order_tiles(L.Rp.n, C.perm.p, L.layR, s);
       if (opt.smoother == SMOOTHER_L1) {
         L.l1.alloc(L.A.n, s);
         BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.val.p, L.A.n,
@@ -455,6 +464,7 @@ void Solver::build_solve_layout() {
   if (own_solve) {
     permute_csr(Aown, lv[0]->perm.p, lv[0]->inv.p, Aownp, s);
     analyze_rows(Aownp, layOwn, s);
+    if (coloured_level(0)) order_tiles(Aownp.n, lv[0]->perm.p, layOwn, s);
   }
   ic.remap(lv[0]->inv.p, s);
   f32_ready = false;
