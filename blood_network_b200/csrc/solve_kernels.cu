@@ -69,8 +69,10 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
     }
     T hold = (MODE == SPMV_Y) ? T(0) : cb;
     if (ce1 - ce0 <= kTileNnz) {
+      // matrix entries are read once: evict-first, so that L2 keeps x
 #pragma unroll 4
-      for (int k = ce0 + threadIdx.x; k < ce1; k += kRows) prod[k - ce0] = dmul(a[k], x[ja[k]]);
+      for (int k = ce0 + threadIdx.x; k < ce1; k += kRows)
+        prod[k - ce0] = dmul(__ldcs(a + k), x[__ldcs(ja + k)]);
       __syncthreads();
       if (i < r1) {
         for (int k = ck0 - ce0; k < ck1 - ce0; k++)

@@ -42,7 +42,7 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
 // of them taken joins the set's overflow class (colour kMaxColors), which the
 // smoother updates Jacobi-style.
 constexpr int kMaxColors = 32;
-constexpr int kCoarseColors = 8;
+constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 is fastest with margin
 constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
@@ -283,7 +283,9 @@ void Solver::color_level(Level& L, int smoother) {
   // join the Jacobi-updated overflow class): each class costs a sequential
   // step per sweep
   const double avg_row = n > 0 ? (double)L.A.nnz / n : 0.0;
-  const int cap = avg_row > 16.0 ? kCoarseColors : kMaxColors;
+  static const int coarse_cap = getenv("BN_COARSE_COLORS") ? atoi(getenv("BN_COARSE_COLORS"))
+                                                            : kCoarseColors;
+  const int cap = avg_row > 16.0 ? coarse_cap : kMaxColors;
   int done = 0, round = 0;
   while (done < n) {
     BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
