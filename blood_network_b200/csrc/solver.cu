@@ -43,6 +43,7 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
 // smoother updates Jacobi-style.
 constexpr int kMaxColors = 32;
 constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 is fastest with margin
+constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than this are capped
 constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
@@ -285,7 +286,8 @@ void Solver::color_level(Level& L, int smoother) {
   const double avg_row = n > 0 ? (double)L.A.nnz / n : 0.0;
   static const int coarse_cap = getenv("BN_COARSE_COLORS") ? atoi(getenv("BN_COARSE_COLORS"))
                                                             : kCoarseColors;
-  const int cap = avg_row > 16.0 ? coarse_cap : kMaxColors;
+  static const double cap_avg = getenv("BN_CAP_AVG") ? atof(getenv("BN_CAP_AVG")) : kCapAvgRow;
+  const int cap = avg_row > cap_avg ? coarse_cap : kMaxColors;
   int done = 0, round = 0;
   while (done < n) {
     BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
