@@ -169,7 +169,11 @@ struct Phase {
   Phase(const char* nm, cudaStream_t st, int lev = -1) : name(nm), s(st), level(lev) {
     if (trace_on()) { cudaStreamSynchronize(s); t0 = wall_seconds(); }
   }
-  ~Phase() {
+  bool live = true;
+  // report now (instead of at the end of the scope)
+  void done() {
+    if (!live) return;
+    live = false;
     if (trace_on()) {
       cudaStreamSynchronize(s);
       if (level >= 0)
@@ -178,6 +182,7 @@ struct Phase {
         fprintf(stderr, "[bn]     %-26s %10.3f ms\n", name, (wall_seconds() - t0) * 1e3);
     }
   }
+  ~Phase() { done(); }
 };
 
 }  // namespace bn

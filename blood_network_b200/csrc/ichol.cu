@@ -623,6 +623,7 @@ void IChol::load(CSR&& Lf, cudaStream_t s) {
 void IChol::finish(const int* aia, const int* aja, const double* aval, bool numeric,
                    cudaStream_t s) {
   const int g = grid_for(n, 256);
+  Phase ph_lower("ichol lower", s);
   DBuf<int> flags(1, s);
   flags.zero();
   pre.alloc(n, s);
@@ -637,9 +638,11 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   BN_REQUIRE(!(f & 1), BN_ERR_ARG, "IC(0): a row has no diagonal entry");
   BN_REQUIRE(!(f & 2), BN_ERR_ARG, "IC(0): factor holds an entry above the diagonal");
 
+  ph_lower.done();
   // strict lower part and its transpose (the dependents of each row)
   CSR Sl, U;
   {
+    Phase ph("ichol strict+transpose", s);
     DBuf<int> c((size_t)n + 1, s);
     c.zero();
     BN_LAUNCH(k_strict_count, g, 256, 0, s, L.ia.p, L.ja.p, n, c.p);
@@ -727,6 +730,7 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   }
 
   // forward solve layout (level order)
+  Phase ph_lay("ichol layouts", s);
   fia.alloc((size_t)n + 1, s);
   fia.zero();
   BN_LAUNCH(k_fwd_count, g, 256, 0, s, L.ia.p, L.ja.p, order.p, n, fia.p);
@@ -747,8 +751,12 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     bsrc.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
     BN_LAUNCH(k_bwd_fill, g, 256, 0, s, U.ia.p, U.ja.p, usrc.p, border.p, n, bia.p, bja.p, bsrc.p);
   }
-  refresh_values();
-  remap(nullptr, s);
+  ph_lay.done();
+  {
+    Phase ph("ichol values", s);
+    refresh_values();
+    remap(nullptr, s);
+  }
   err.alloc(1, s);  // here, never inside a stream capture
   err.zero();
 }

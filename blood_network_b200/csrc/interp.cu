@@ -65,10 +65,75 @@ __device__ __forceinline__ int strong_slot(const int* __restrict__ sja, int s0, 
   return -1;
 }
 
+// Hub rows of A (longer than kInterpHub entries) get a column -> entry
+// index hash table (open addressing, at most half full, so every probe
+// sequence ends at an empty slot).  A row whose strong F neighbour is a hub
+// then finds the entries of its own strong C points in that row by lookup
+// instead of walking the hub's row, and visits them in row order -- the
+// same entries, in the same order, as the walk.
+constexpr int kInterpHub = 512;
+constexpr int kInterpMaxC = 32;  // rows with more strong C points keep the walk
+
+__device__ __forceinline__ unsigned hub_hash(int m) { return (unsigned)m * 2654435761u; }
+
+__global__ void k_hub_mark(const int* __restrict__ aia, int n, int* __restrict__ hubidx,
+                           int* __restrict__ hubrows, int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int h = -1;
+    if (aia[i + 1] - aia[i] > kInterpHub) {
+      h = atomicAdd(counter, 1);
+      hubrows[h] = i;
+    }
+    hubidx[i] = h;
+  }
+}
+
+__global__ void k_hub_size(const int* __restrict__ aia, const int* __restrict__ hubrows, int nh,
+                           int* __restrict__ hsz) {
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += gridDim.x * blockDim.x) {
+    const int len = aia[hubrows[h] + 1] - aia[hubrows[h]];
+    int sz = 1;
+    while (sz < 2 * len) sz <<= 1;
+    hsz[h] = sz;
+  }
+}
+
+__global__ void k_hub_fill(const int* __restrict__ aia, const int* __restrict__ aja,
+                           const int* __restrict__ hubrows, const int* __restrict__ hoff,
+                           int* __restrict__ keys, int* __restrict__ vals) {
+  const int h = blockIdx.x;
+  const int i = hubrows[h];
+  const int off = hoff[h], mask = hoff[h + 1] - off - 1;
+  for (int l = aia[i] + threadIdx.x; l < aia[i + 1]; l += blockDim.x) {
+    const int m = aja[l];
+    int slot = (int)(hub_hash(m) & (unsigned)mask);
+    while (true) {
+      const int prev = atomicCAS(&keys[off + slot], -1, m);
+      if (prev == -1) { vals[off + slot] = l; break; }
+      slot = (slot + 1) & mask;
+    }
+  }
+}
+
+// entry index of column m in hub row h, or -1
+__device__ __forceinline__ int hub_find(const int* __restrict__ keys, const int* __restrict__ vals,
+                                        const int* __restrict__ hoff, int h, int m) {
+  const int off = hoff[h], mask = hoff[h + 1] - off - 1;
+  int slot = (int)(hub_hash(m) & (unsigned)mask);
+  while (true) {
+    const int k = keys[off + slot];
+    if (k == m) return vals[off + slot];
+    if (k == -1) return -1;
+    slot = (slot + 1) & mask;
+  }
+}
+
 __global__ void k_interp_values(const int* __restrict__ aia, const int* __restrict__ aja,
                                 const double* __restrict__ aval, const int* __restrict__ sia,
                                 const int* __restrict__ sja, const int* __restrict__ cf, int n,
-                                const int* __restrict__ pia, double* __restrict__ pval) {
+                                const int* __restrict__ pia, double* __restrict__ pval,
+                                const int* __restrict__ hubidx, const int* __restrict__ hoff,
+                                const int* __restrict__ hkeys, const int* __restrict__ hvals) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int p0 = pia[i], p1 = pia[i + 1];
     if (cf[i] == 1) {
@@ -95,6 +160,18 @@ __global__ void k_interp_values(const int* __restrict__ aia, const int* __restri
         weak = xadd(weak, a);
     }
     double diag_hat = xadd(diag, weak);
+    // this row's strong C points in S order (slot q = index in the list)
+    int cm[kInterpMaxC];
+    int nc = 0;
+    if (hubidx) {
+      for (int k = s0; k < s1 && nc <= kInterpMaxC; k++) {
+        const int q = sja[k];
+        if (cf[q] == 1) {
+          if (nc < kInterpMaxC) cm[nc] = q;
+          nc++;
+        }
+      }
+    }
     for (int k = aia[i]; k < aia[i + 1]; k++) {
       int kk = aja[k];
       if (kk == i) continue;
@@ -102,6 +179,33 @@ __global__ void k_interp_values(const int* __restrict__ aia, const int* __restri
       strong_slot(sja, s0, s1, cf, kk, &strong);
       if (!strong || cf[kk] != -1) continue;
       const double a_ik = aval[k];
+      const int h = hubidx ? hubidx[kk] : -1;
+      if (h >= 0 && nc <= kInterpMaxC) {
+        // entries of row kk in C_i, by lookup, then in row order
+        int el[kInterpMaxC], sl[kInterpMaxC];
+        int ne = 0;
+        for (int q = 0; q < nc; q++) {
+          const int l = hub_find(hkeys, hvals, hoff, h, cm[q]);
+          if (l < 0) continue;
+          int t = ne++;
+          while (t > 0 && el[t - 1] > l) {
+            el[t] = el[t - 1];
+            sl[t] = sl[t - 1];
+            t--;
+          }
+          el[t] = l;
+          sl[t] = q;
+        }
+        double denom = 0.0;
+        for (int t = 0; t < ne; t++) denom = xadd(denom, aval[el[t]]);
+        if (fabs(denom) < 1e-15) {
+          diag_hat = xadd(diag_hat, a_ik);
+        } else {
+          for (int t = 0; t < ne; t++)
+            pval[p0 + sl[t]] = xadd(pval[p0 + sl[t]], xdiv(xmul(a_ik, aval[el[t]]), denom));
+        }
+        continue;
+      }
       double denom = 0.0;
       for (int l = aia[kk]; l < aia[kk + 1]; l++) {
         int m = aja[l];
@@ -131,8 +235,24 @@ __global__ void k_interp_values(const int* __restrict__ aia, const int* __restri
 
 void interpolation_values(const CSR& A, const CSR& S, const int* cf, CSR& P, cudaStream_t s) {
   if (A.n == 0) return;
-  BN_LAUNCH(k_interp_values, grid_for(A.n, 128), 128, 0, s, A.ia.p, A.ja.p, A.val.p, S.ia.p,
-            S.ja.p, cf, A.n, P.ia.p, P.val.p);
+  const int n = A.n;
+  DBuf<int> hubidx(n, s), hubrows(n, s), ctr(1, s);
+  ctr.zero();
+  BN_LAUNCH(k_hub_mark, grid_for(n, 256), 256, 0, s, A.ia.p, n, hubidx.p, hubrows.p, ctr.p);
+  const int nh = read_scalar(ctr.p, s);
+  DBuf<int> hoff((size_t)nh + 1, s), keys, vals;
+  if (nh > 0) {
+    hoff.zero();
+    BN_LAUNCH(k_hub_size, grid_for(nh, 256), 256, 0, s, A.ia.p, hubrows.p, nh, hoff.p);
+    const int tot = scan_counts(hoff.p, nh, s);
+    keys.alloc(tot, s);
+    vals.alloc(tot, s);
+    keys.fill_bytes(0xff);
+    BN_LAUNCH(k_hub_fill, nh, 256, 0, s, A.ia.p, A.ja.p, hubrows.p, hoff.p, keys.p, vals.p);
+  }
+  BN_LAUNCH(k_interp_values, grid_for(n, 128), 128, 0, s, A.ia.p, A.ja.p, A.val.p, S.ia.p,
+            S.ja.p, cf, n, P.ia.p, P.val.p, nh > 0 ? hubidx.p : nullptr, hoff.p, keys.p,
+            vals.p);
 }
 
 void interpolation_pattern(const CSR& S, const int* cf, int n_coarse, CSR& P, cudaStream_t s) {

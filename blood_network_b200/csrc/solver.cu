@@ -44,6 +44,7 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
 constexpr int kMaxColors = 32;
 constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 is fastest with margin
 constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than this are capped
+constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
@@ -78,6 +79,11 @@ __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict_
     }
   }
   if (local) atomicAdd(counter, local);
+}
+
+__global__ void k_color_rest(int n, int* __restrict__ color) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (color[i] < 0) color[i] = kMaxColors;
 }
 
 __global__ void k_color_commit(int n, const int* __restrict__ newc, int* __restrict__ color) {
@@ -288,9 +294,17 @@ void Solver::color_level(Level& L, int smoother) {
                                                             : kCoarseColors;
   static const double cap_avg = getenv("BN_CAP_AVG") ? atof(getenv("BN_CAP_AVG")) : kCapAvgRow;
   const int cap = avg_row > cap_avg ? coarse_cap : kMaxColors;
+  // capped levels: rows still uncoloured after kCappedRounds rounds join
+  // the overflow class
+  static const int capped_rounds =
+      getenv("BN_CAP_ROUNDS") ? atoi(getenv("BN_CAP_ROUNDS")) : kCappedRounds;
   int done = 0, round = 0;
   while (done < n) {
     BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
+    if (cap < kMaxColors && round >= capped_rounds) {
+      BN_LAUNCH(k_color_rest, g, 256, 0, s, n, color.p);
+      break;
+    }
     ctr.zero();
     BN_LAUNCH(k_color_round, g, 256, 0, s, L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, n,
               color.p, newc.p, ctr.p, cap);
@@ -438,22 +452,23 @@ void Solver::build_solve_layout() {
         BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.val.p, L.A.n,
                   L.l1.p);
       }
-      if (use_packed) {
+      if (use_packed) {  // packings only for the operators that run on them
         Phase ph2("packing", s, l);
-        std::vector<int> ha = host_ia(L.Ap, s);
-        L.pkA.build(ha, {make_int2(0, L.Ap.n)}, s);
-        if (coloured_level(l)) {
-          std::vector<int2> rg;
-          for (size_t c = 0; c + 1 < L.cptr.size(); c++) rg.push_back(make_int2(L.cptr[c], L.cptr[c + 1]));
-          L.pkG.build(ha, rg, s);
-        }
-        std::vector<int> hp = host_ia(L.Pp, s);
-        L.pkP.build(hp, {make_int2(0, L.Pp.n)}, s);
-        std::vector<int> hr = host_ia(L.Rp, s);
-        L.pkR.build(hr, {make_int2(0, L.Rp.n)}, s);
         L.use_pkA = L.layA.nlong > 0;
         L.use_pkP = L.layP.nlong > 0;
         L.use_pkR = L.layR.nlong > 0;
+        if (L.use_pkA) {
+          std::vector<int> ha = host_ia(L.Ap, s);
+          L.pkA.build(ha, {make_int2(0, L.Ap.n)}, s);
+          if (coloured_level(l)) {
+            std::vector<int2> rg;
+            for (size_t c = 0; c + 1 < L.cptr.size(); c++)
+              rg.push_back(make_int2(L.cptr[c], L.cptr[c + 1]));
+            L.pkG.build(ha, rg, s);
+          }
+        }
+        if (L.use_pkP) L.pkP.build(host_ia(L.Pp, s), {make_int2(0, L.Pp.n)}, s);
+        if (L.use_pkR) L.pkR.build(host_ia(L.Rp, s), {make_int2(0, L.Rp.n)}, s);
         if (trace_on())
           fprintf(stderr, "[bn] L%d packed kernels: A %d (%d long rows)  P %d  R %d (%d long rows)\n",
                   l, (int)L.use_pkA, L.layA.nlong, (int)L.use_pkP, (int)L.use_pkR, L.layR.nlong);
