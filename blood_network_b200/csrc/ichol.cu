@@ -138,6 +138,49 @@ __global__ void k_kahn_step(const int* __restrict__ uia, const int* __restrict__
   }
 }
 
+// The whole sweep in one cooperative launch: each step releases the
+// dependents of the current frontier [lo, hi); a grid barrier, then every
+// thread reads the new end, then a second barrier before the next step
+// appends to the frontier again.  Levels are fixed by the dependency graph;
+// only the order inside a frontier depends on timing, and the rows are
+// later sorted stably by level.
+__global__ void k_kahn_all(const int* __restrict__ uia, const int* __restrict__ uja, int n,
+                           int* __restrict__ indeg, int* __restrict__ level,
+                           int* __restrict__ frontier, int* counter, int* nlev) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gsz = gridDim.x * blockDim.x;
+  int lo = 0;
+  int hi = *(volatile int*)counter;
+  int lev = 0;
+  while (hi > lo && lev < n) {
+    lev++;
+    for (int t = lo + gtid; t < hi; t += gsz) {
+      const int k = frontier[t];
+      for (int q = uia[k]; q < uia[k + 1]; q++) {
+        const int i = uja[q];
+        if (atomicSub(&indeg[i], 1) == 1) {
+          level[i] = lev;
+          frontier[atomicAdd(counter, 1)] = i;
+        }
+      }
+    }
+    grid.sync();
+    lo = hi;
+    hi = *(volatile int*)counter;
+    grid.sync();
+  }
+  if (gtid == 0) *nlev = lev;
+}
+
+__global__ void k_level_starts(const int* __restrict__ lev, int n, int nlevels,
+                               int* __restrict__ ptr) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    if (t == 0 || lev[t] != lev[t - 1]) ptr[lev[t]] = t;
+  if (blockIdx.x == 0 && threadIdx.x == 0) ptr[nlevels] = n;
+}
+
 __global__ void k_iota_i(int* a, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
 }
@@ -663,17 +706,33 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     DBuf<int> indeg(n, s), level(n, s), frontier(n, s), ctr(1, s);
     ctr.zero();
     BN_LAUNCH(k_indeg, g, 256, 0, s, Sl.ia.p, n, indeg.p, level.p, frontier.p, ctr.p);
-    int lo = 0, hi = read_scalar(ctr.p, s);
-    int lev = 0;
-    while (hi > lo) {
-      lev++;
-      BN_LAUNCH(k_kahn_step, grid_for(hi - lo, 256), 256, 0, s, U.ia.p, U.ja.p, frontier.p + lo,
-                hi - lo, lev, indeg.p, level.p, frontier.p, ctr.p);
-      lo = hi;
-      hi = read_scalar(ctr.p, s);
+    {  // all Kahn steps in one cooperative launch
+      DBuf<int> nlev(1, s);
+      int dev = 0, per_sm = 0, sms = 0;
+      BN_CUDA(cudaGetDevice(&dev));
+      BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kahn_all, 256, 0));
+      BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      const int grid = sms * (per_sm < 4 ? per_sm : 4);
+      BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): level sweep grid does not fit");
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(grid);
+      cfg.blockDim = dim3(256);
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      g_launch_count++;
+      int* uia = U.ia.p;
+      int* uja = U.ja.p;
+      BN_CUDA(cudaLaunchKernelEx(&cfg, k_kahn_all, (const int*)uia, (const int*)uja, n, indeg.p,
+                                 level.p, frontier.p, ctr.p, nlev.p));
+      const int reached = read_scalar(ctr.p, s);
+      BN_REQUIRE(reached == n, BN_ERR_ARG, "IC(0): dependency levels did not cover every row");
+      // one step per level; the last one finds no new rows
+      nlevels = read_scalar(nlev.p, s);
     }
-    BN_REQUIRE(hi == n, BN_ERR_ARG, "IC(0): dependency levels did not cover every row");
-    nlevels = lev;
     // level order, stable (natural order within a level)
     order.alloc(n, s);
     DBuf<int> ids(n, s), keys_out(n, s);
@@ -686,13 +745,12 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     DBuf<unsigned char> t(tmp, s);
     BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, level.p, keys_out.p, ids.p, order.p, n, 0,
                                             eb, s));
-    // level offsets
-    std::vector<int> hk(n);
-    keys_out.download(hk.data(), n);
-    BN_CUDA(cudaStreamSynchronize(s));
+    // level offsets from the sorted levels (every level holds a row)
+    DBuf<int> dptr((size_t)nlevels + 1, s);
+    BN_LAUNCH(k_level_starts, g, 256, 0, s, keys_out.p, n, nlevels, dptr.p);
     lptr.assign(nlevels + 1, 0);
-    for (int i = 0; i < n; i++) lptr[hk[i] + 1]++;
-    for (int l = 0; l < nlevels; l++) lptr[l + 1] += lptr[l];
+    dptr.download(lptr.data(), (size_t)nlevels + 1);
+    BN_CUDA(cudaStreamSynchronize(s));
   }
   // backward processing order: reverse level order
   border.alloc(n, s);

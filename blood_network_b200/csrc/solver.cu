@@ -45,15 +45,17 @@ constexpr int kMaxColors = 32;
 constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 is fastest with margin
 constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than this are capped
 constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
+constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
 constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
                               const int* __restrict__ set, int n, const int* __restrict__ color,
-                              int* __restrict__ newc, int* counter, int cap) {
+                              int* __restrict__ newc, int* counter, int cap, int long_len) {
   int local = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     newc[i] = -1;
     if (color[i] >= 0) continue;
+    if (ia[i + 1] - ia[i] > long_len) continue;  // k_color_round_long
     // priority: row length first (dense rows decide early), hash second
     const unsigned long long pi =
         ((unsigned long long)(ia[i + 1] - ia[i]) << 32) | color_hash((unsigned)i);
@@ -79,6 +81,68 @@ __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict_
     }
   }
   if (local) atomicAdd(counter, local);
+}
+
+// The same round for the long rows, one warp per row: the outcome (local
+// maximum or not, colours in use) does not depend on the visiting order.
+__global__ void k_color_round_long(const int* __restrict__ ia, const int* __restrict__ ja,
+                                   const int* __restrict__ set, const int* __restrict__ lrows,
+                                   int nl, const int* __restrict__ color, int* __restrict__ newc,
+                                   int* counter, int cap) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nl; w += warps) {
+    const int i = lrows[w];
+    if (color[i] >= 0) continue;
+    const unsigned long long pi =
+        ((unsigned long long)(ia[i + 1] - ia[i]) << 32) | color_hash((unsigned)i);
+    const int si = set ? set[i] : 0;
+    unsigned used = 0;
+    bool blocked = false;
+    for (int k0 = ia[i]; k0 < ia[i + 1]; k0 += 32) {
+      const int k = k0 + lane;
+      if (k < ia[i + 1]) {
+        const int j = ja[k];
+        if (j != i && !(set && set[j] != si)) {
+          const int cj = color[j];
+          if (cj >= 0) {
+            if (cj < kMaxColors) used |= 1u << cj;
+          } else if ((((unsigned long long)(ia[j + 1] - ia[j]) << 32) |
+                      color_hash((unsigned)j)) > pi) {
+            blocked = true;
+          }
+        }
+      }
+      if (__any_sync(0xffffffffu, blocked)) break;
+    }
+    blocked = __any_sync(0xffffffffu, blocked);
+    used = __reduce_or_sync(0xffffffffu, used);
+    if (lane == 0 && !blocked) {
+      const int c = (used == 0xffffffffu) ? kMaxColors : __ffs(~used) - 1;
+      newc[i] = c < cap ? c : kMaxColors;
+      atomicAdd(counter, 1);
+    }
+  }
+}
+
+__global__ void k_class_counts(const int* __restrict__ key, int n, int* __restrict__ cnt) {
+  __shared__ int h[256];
+  for (int q = threadIdx.x; q < 256; q += blockDim.x) h[q] = 0;
+  __syncthreads();
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int cls = key[t] >> 1;
+    atomicAdd(&h[cls], 1);
+    if (key[t] & 1) atomicAdd(&h[128 + cls], 1);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < 256; q += blockDim.x)
+    if (h[q]) atomicAdd(&cnt[q], h[q]);
+}
+
+__global__ void k_long_list(const int* __restrict__ ia, int n, int long_len,
+                            int* __restrict__ lrows, int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (ia[i + 1] - ia[i] > long_len) lrows[atomicAdd(counter, 1)] = i;
 }
 
 __global__ void k_color_rest(int n, int* __restrict__ color) {
@@ -298,6 +362,11 @@ void Solver::color_level(Level& L, int smoother) {
   // the overflow class
   static const int capped_rounds =
       getenv("BN_CAP_ROUNDS") ? atoi(getenv("BN_CAP_ROUNDS")) : kCappedRounds;
+  // long rows (order of the list is irrelevant: each row's outcome is)
+  DBuf<int> lrows(n > 0 ? n : 1, s), lctr(1, s);
+  lctr.zero();
+  if (n > 0) BN_LAUNCH(k_long_list, g, 256, 0, s, L.A.ia.p, n, kColorLong, lrows.p, lctr.p);
+  const int nlong_rows = read_scalar(lctr.p, s);
   int done = 0, round = 0;
   while (done < n) {
     BN_REQUIRE(round <= n, BN_ERR_ARG, "colouring did not finish");
@@ -307,7 +376,11 @@ void Solver::color_level(Level& L, int smoother) {
     }
     ctr.zero();
     BN_LAUNCH(k_color_round, g, 256, 0, s, L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, n,
-              color.p, newc.p, ctr.p, cap);
+              color.p, newc.p, ctr.p, cap, kColorLong);
+    if (nlong_rows > 0)
+      BN_LAUNCH(k_color_round_long, grid_for((long long)nlong_rows * 32, 256), 256, 0, s,
+                L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, lrows.p, nlong_rows, color.p,
+                newc.p, ctr.p, cap);
     BN_LAUNCH(k_color_commit, g, 256, 0, s, n, newc.p, color.p);
     done += read_scalar(ctr.p, s);
     round++;
@@ -322,22 +395,23 @@ void Solver::color_level(Level& L, int smoother) {
   DBuf<unsigned char> t(tmp, s);
   BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, key.p, key_out.p, ids.p, L.gs_rows.p, n, 0, 8,
                                           s));
-  std::vector<int> hk(n);
-  key_out.download(hk.data(), n);
+  // class sizes and long-row counts per class id (key >> 1 < 128); the
+  // sorted rows hold the classes in ascending id order
+  DBuf<int> ccnt(256, s);
+  ccnt.zero();
+  if (n > 0) BN_LAUNCH(k_class_counts, g, 256, 0, s, key_out.p, n, ccnt.p);
+  std::vector<int> hc(256);
+  ccnt.download(hc.data(), 256);
   BN_CUDA(cudaStreamSynchronize(s));
   L.cptr.clear();
   L.cjac.clear();
   L.clong.clear();
   L.cptr.push_back(0);
-  int nlong = 0;
-  for (int i = 1; i <= n; i++) {
-    nlong += (hk[i - 1] & 1);
-    if (i == n || (hk[i] >> 1) != (hk[i - 1] >> 1)) {
-      L.cptr.push_back(i);
-      L.cjac.push_back(((hk[i - 1] >> 1) & 63) == kMaxColors ? 1 : 0);
-      L.clong.push_back(nlong);
-      nlong = 0;
-    }
+  for (int cls = 0; cls < 128; cls++) {
+    if (hc[cls] == 0) continue;
+    L.cptr.push_back(L.cptr.back() + hc[cls]);
+    L.cjac.push_back((cls & 63) == kMaxColors ? 1 : 0);
+    L.clong.push_back(hc[128 + cls]);
   }
   L.colored_for = smoother;
   L.color_rounds = round;
