@@ -72,7 +72,36 @@ __device__ __forceinline__ int table_slot(Table t, int key, int new_slot, bool* 
   }
 }
 
-// product-count bound per coarse row: 1 (diagonal) + sum |P_i2|
+// product-count bound per coarse row: 1 (diagonal) + sum |P_i2| over the
+// entries i2 of the A rows i1 of R's row, computed as 1 + sum_{i1} w_{i1}
+// with w_{i1} = sum_{i2 in A_{i1}} |P_{i2}| (one pass over A, one over R)
+__global__ void k_fine_weights(const int* __restrict__ aia, const int* __restrict__ aja,
+                               const int* __restrict__ pia, int n, long long* __restrict__ w) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i1 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i1 < n; i1 += warps) {
+    long long b = 0;
+    for (int k2 = aia[i1] + lane; k2 < aia[i1 + 1]; k2 += 32) {
+      const int i2 = aja[k2];
+      b += pia[i2 + 1] - pia[i2];
+    }
+    for (int off = 16; off > 0; off >>= 1) b += __shfl_xor_sync(0xffffffffu, b, off);
+    if (lane == 0) w[i1] = b;
+  }
+}
+
+__global__ void k_rap_bound_w(const int* __restrict__ ria, const int* __restrict__ rja,
+                              const long long* __restrict__ w, int nc, long long* __restrict__ ub) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int ic = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ic < nc; ic += warps) {
+    long long b = 0;
+    for (int k1 = ria[ic] + lane; k1 < ria[ic + 1]; k1 += 32) b += w[rja[k1]];
+    for (int off = 16; off > 0; off >>= 1) b += __shfl_xor_sync(0xffffffffu, b, off);
+    if (lane == 0) ub[ic] = 1 + b;
+  }
+}
+
 __global__ void k_rap_bound(const int* __restrict__ ria, const int* __restrict__ rja,
                             const int* __restrict__ aia, const int* __restrict__ aja,
                             const int* __restrict__ pia, int nc, long long* __restrict__ ub) {
@@ -332,6 +361,7 @@ __global__ void k_rap_fill_huge(const int* __restrict__ ria, const int* __restri
 // exactly as the reference), and the columns are put back in order of first
 // appearance, which places the diagonal first.
 constexpr long long kSortProducts = 16384;
+constexpr long long kLongSeg = 256;  // segments longer than this are summed by a warp
 
 // products per (hub row, R entry) pair: sum over A row i1 of |P_i2|
 __global__ void k_pair_counts(const int* __restrict__ ria, const int* __restrict__ rja,
@@ -482,11 +512,83 @@ __global__ void k_seg_sum(const unsigned long long* __restrict__ keys,
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
        g += (long long)gridDim.x * blockDim.x) {
     const long long b = seg[g], e = (g + 1 < nseg) ? seg[g + 1] : T;
+    if (e - b > kLongSeg) continue;  // k_seg_sum_long
     double v = svals[b];
+#pragma unroll 8
     for (long long p = b + 1; p < e; p++) v = xadd(v, svals[p]);
     sval[g] = v;
     scol[g] = (int)(keys[b] & 0xffffffffull);
     sfirst[g] = idx[b];
+  }
+}
+
+// long segments, one warp each: the warp loads the next kSegChunk products
+// (coalesced, into registers) while lane 0 adds the current chunk from
+// shared memory in stream order; the loads' latency hides behind the adds.
+constexpr int kSegChunk = 256;
+__global__ void __launch_bounds__(32)
+k_seg_sum_long(const unsigned long long* __restrict__ keys, const long long* __restrict__ idx,
+               const double* __restrict__ svals, const long long* __restrict__ seg,
+               long long nseg, long long T, const long long* __restrict__ lsegs, int nl,
+               double* __restrict__ sval, int* __restrict__ scol,
+               long long* __restrict__ sfirst) {
+  __shared__ double buf[2][kSegChunk];
+  const int lane = threadIdx.x;
+  constexpr int kPer = kSegChunk / 32;
+  for (int w = blockIdx.x; w < nl; w += gridDim.x) {
+    const long long g = lsegs[w];
+    const long long b = seg[g], e = (g + 1 < nseg) ? seg[g + 1] : T;
+    double x[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; r++) {
+      const long long q = b + r * 32 + lane;
+      x[r] = q < e ? svals[q] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < kPer; r++) buf[0][r * 32 + lane] = x[r];
+    __syncwarp();
+    double v = 0.0;
+    int slot = 0;
+    for (long long p0 = b; p0 < e; p0 += kSegChunk) {
+      const long long pn = p0 + kSegChunk;
+      if (pn < e) {
+#pragma unroll
+        for (int r = 0; r < kPer; r++) {
+          const long long q = pn + r * 32 + lane;
+          x[r] = q < e ? svals[q] : 0.0;
+        }
+      }
+      if (lane == 0) {
+        const int cnt = e - p0 < kSegChunk ? (int)(e - p0) : kSegChunk;
+        int q0 = 0;
+        if (p0 == b) { v = buf[slot][0]; q0 = 1; }
+#pragma unroll 8
+        for (int q = q0; q < cnt; q++) v = xadd(v, buf[slot][q]);
+      }
+      __syncwarp();
+      if (pn < e) {
+#pragma unroll
+        for (int r = 0; r < kPer; r++) buf[slot ^ 1][r * 32 + lane] = x[r];
+      }
+      __syncwarp();
+      slot ^= 1;
+    }
+    if (lane == 0) {
+      sval[g] = v;
+      scol[g] = (int)(keys[b] & 0xffffffffull);
+      sfirst[g] = idx[b];
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void k_long_segs(const long long* __restrict__ seg, long long nseg, long long T,
+                            long long* __restrict__ out, int* counter) {
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nseg;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long e = (g + 1 < nseg) ? seg[g + 1] : T;
+    if (e - seg[g] > kLongSeg) out[atomicAdd(counter, 1)] = g;
+    atomicMax(counter + 1, (int)(e - seg[g] < 0x7fffffff ? e - seg[g] : 0x7fffffff));
   }
 }
 
@@ -598,6 +700,9 @@ static void hub_prepare(const CSR& R, const CSR& A, const CSR& P, const int* row
 static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
   const long long nseg = H.nseg, T = H.T;
   const int m = H.m;
+  if (trace_on())
+    fprintf(stderr, "[bn]     hub rows %d products %lld columns %lld\n", m, T, nseg);
+  Phase ph1("hub sums", s);
   DBuf<long long> rowseg((size_t)m + 1, s);
   rowseg.zero();
   BN_LAUNCH(k_rows_seglen, grid_for(m, 128), 128, 0, s, rows, m, Ac.ia.p, rowseg.p);
@@ -610,6 +715,21 @@ static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
   BN_LAUNCH(k_gather_sorted, grid_for(T, 256), 256, 0, s, H.idx2.p, T, H.vals.p, svals.p);
   BN_LAUNCH(k_seg_sum, grid_for(nseg, 128), 128, 0, s, H.keys2.p, H.idx2.p, svals.p, H.seg.p,
             nseg, T, sval.p, scol.p, sfirst.p);
+  {
+    DBuf<long long> lsegs(nseg, s);
+    DBuf<int> lc(2, s);
+    lc.zero();
+    BN_LAUNCH(k_long_segs, grid_for(nseg, 256), 256, 0, s, H.seg.p, nseg, T, lsegs.p, lc.p);
+    const int nl = read_scalar(lc.p, s);
+    if (trace_on())
+      fprintf(stderr, "[bn]     hub columns over %lld products: %d, longest %d\n", kLongSeg, nl,
+              read_scalar(lc.p + 1, s));
+    if (nl > 0)
+      BN_LAUNCH(k_seg_sum_long, nl < 32768 ? nl : 32768, 32, 0, s, H.keys2.p, H.idx2.p, svals.p,
+                H.seg.p, nseg, T, lsegs.p, nl, sval.p, scol.p, sfirst.p);
+  }
+  ph1.done();
+  Phase ph2("hub reorder+write", s);
   BN_LAUNCH(k_seg_rowkeys, grid_for(nseg, 256), 256, 0, s, H.keys2.p, H.seg.p, nseg, srow.p);
   BN_LAUNCH(k_iota64, grid_for(nseg, 256), 256, 0, s, g_in.p, nseg);
   int fb = 1;
@@ -695,9 +815,14 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
   DBuf<int> cnt((size_t)nc + 1, s), hub(nc > 0 ? nc : 1, s), nh(1, s);
   cnt.zero();
   nh.zero();
+  Phase ph_bound("rap bound", s);
   if (nc > 0) {
-    BN_LAUNCH(k_rap_bound, grid_for((long long)nc * 32, 256, 16), 256, 0, s, R.ia.p, R.ja.p,
-              A.ia.p, A.ja.p, P.ia.p, nc, ub.p);
+    DBuf<long long> w(A.n > 0 ? A.n : 1, s);
+    if (A.n > 0)
+      BN_LAUNCH(k_fine_weights, grid_for((long long)A.n * 32, 256, 16), 256, 0, s, A.ia.p,
+                A.ja.p, P.ia.p, A.n, w.p);
+    BN_LAUNCH(k_rap_bound_w, grid_for((long long)nc * 32, 256, 16), 256, 0, s, R.ia.p, R.ja.p,
+              w.p, nc, ub.p);
     BN_LAUNCH(k_rap_split_hubs, grid_for(nc, 256), 256, 0, s, ub.p, ub.p, nc, est.p, hub.p, nh.p);
   }
   const int nhub = read_scalar(nh.p, s);
@@ -709,6 +834,7 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
     BN_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, hub.p, t_out.p, nhub, 0, 32, s));
     BN_CUDA(cudaMemcpyAsync(hub.p, t_out.p, sizeof(int) * nhub, cudaMemcpyDeviceToDevice, s));
   }
+  ph_bound.done();
   HubStream H;
   // ---- pass 1: count; hub rows from their sorted streams, the rest
   // classified by min(bound, nc)
@@ -722,6 +848,7 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
     const int* L0 = rc.lists.p;
     const int* L1 = rc.lists.p + nc;
     const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    Phase ph("rap count", s);
     if (rc.count[0])
       BN_LAUNCH(k_rap_count_warp, grid_for(rc.count[0], kRapWarps, 64), 32 * kRapWarps, 0, s,
                 R.ia.p, R.ja.p, A.ia.p, A.ja.p, P.ia.p, P.ja.p, L0, rc.count[0], cnt.p);
@@ -764,14 +891,22 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
     const int* L0 = rc.lists.p;
     const int* L1 = rc.lists.p + nc;
     const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    if (trace_on())
+      fprintf(stderr, "[bn]     rap fill classes: warp %d big %d huge %d hubs %d\n", rc.count[0],
+              rc.count[1], rc.count[2], nhub);
+    Phase ph_w("rap fill warp", s);
     if (rc.count[0])
       BN_LAUNCH(k_rap_fill_warp, grid_for(rc.count[0], kRapWarps, 32), 32 * kRapWarps,
                 kWarpFillSmem, s, R.ia.p, R.ja.p, R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p,
                 P.ja.p, P.val.p, L0, rc.count[0], Ac.ia.p, Ac.ja.p, Ac.val.p);
+    ph_w.done();
+    Phase ph_b("rap fill big", s);
     if (rc.count[1])
       BN_LAUNCH(k_rap_fill_big, grid_for(rc.count[1], 1, 2), 32, kBigFillSmem, s, R.ia.p, R.ja.p,
                 R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, L1, rc.count[1],
                 Ac.ia.p, Ac.ja.p, Ac.val.p);
+    ph_b.done();
+    Phase ph_h("rap fill huge", s);
     if (rc.count[2]) {
       const int m = rc.count[2];
       DBuf<long long> toff((size_t)m + 1, s);
