@@ -60,6 +60,25 @@ class IcholFactor(C.Structure):
                 ("val", C.POINTER(C.c_double)), ("nnz", C.c_int)]
 
 
+class AmgLevel(C.Structure):
+    """The reference's amg_level (C_amg1/include/amg.h:42-54)."""
+    _fields_ = [("A", DcsrMat), ("P", DcsrMat), ("A_filtered", DcsrMat),
+                ("mis", C.POINTER(C.c_int)), ("isolated", C.POINTER(C.c_int)),
+                ("cf_order", C.POINTER(C.c_int)), ("n", C.c_int), ("n_coarse", C.c_int),
+                ("L_ichol", IcholFactor), ("l1_diag", C.POINTER(C.c_double))]
+
+
+class AmgData(C.Structure):
+    """The reference's amg_data (C_amg1/include/amg.h:57-71)."""
+    _fields_ = [("levels", AmgLevel * 20), ("num_levels", C.c_int), ("threshold", C.c_double),
+                ("min_size", C.c_int), ("max_levels", C.c_int), ("maxit_prol", C.c_int),
+                ("lump", C.c_int), ("nu", C.c_int), ("smoother", C.c_int),
+                ("omega_jacobi", C.c_double), ("coarsening", C.c_int)]
+
+
+# void (*precond)(const void* data, const double* g, double* Bg)
+PRECOND_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
+
 _lib = None
 
 
@@ -112,6 +131,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ichol_solve": (None, [C.POINTER(IcholFactor), vp, vp]),
         "ichol_free": (None, [C.POINTER(IcholFactor)]),
         "ichol_solve_noalloc": (i, [i, vp, vp, vp, vp, vp, vp]),
+        "amg_build_hierarchy": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat)]),
+        "amg_rebuild_values": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat)]),
+        "amg_free": (None, [C.POINTER(AmgData)]),
+        "amg_backslash": (None, [C.POINTER(AmgData), i, vp, vp, i]),
+        "amg_fwdslash": (None, [C.POINTER(AmgData), i, vp, vp, i]),
+        "amg_vcycle_precond": (None, [C.POINTER(AmgData), vp, vp]),
+        "amg_ichol_precond": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat),
+                                     C.POINTER(IcholFactor), vp, vp]),
+        "amg_pcg": (i, [C.POINTER(DcsrMat), vp, vp, PRECOND_FN, vp, d, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -128,7 +156,7 @@ def exported_symbols():
     text = open(hdr).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     names = re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", text)
-    skip = {"if", "for", "while", "return", "sizeof", "defined"}
+    skip = {"if", "for", "while", "return", "sizeof", "defined", "void"}  # void (*fn)(...)
     return sorted({n for n in names if n not in skip})
 
 

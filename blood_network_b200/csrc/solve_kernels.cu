@@ -543,6 +543,22 @@ void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double*
   BN_LAUNCH(k_dot2<T>, kRedBlocks, 256, 0, s, u, v, w, n, p0, p1);
 }
 
+// y += a u ;  p = z + b p   (uuplmv / umuplv of vector_ops.c with a host scalar)
+__global__ void k_axpy(double* __restrict__ y, const double* __restrict__ u, double a, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = y[i] + u[i] * a;
+}
+__global__ void k_xpby(double* __restrict__ p, const double* __restrict__ z, double b, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = z[i] + p[i] * b;
+}
+void vaxpy(double* y, const double* u, double a, int n, cudaStream_t s) {
+  if (n > 0) BN_LAUNCH(k_axpy, grid_for(n, 256), 256, 0, s, y, u, a, n);
+}
+void vxpby(double* p, const double* z, double b, int n, cudaStream_t s) {
+  if (n > 0) BN_LAUNCH(k_xpby, grid_for(n, 256), 256, 0, s, p, z, b, n);
+}
+
 // Reduce a partial array into slot `dst` of the scalar block.
 __global__ void k_reduce(const double* __restrict__ part, int m, double* __restrict__ out) {
   __shared__ double red[32];

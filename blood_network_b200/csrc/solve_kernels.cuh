@@ -96,6 +96,8 @@ template <class T>
 void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double* p1,
                   cudaStream_t s);
 void reduce_partials(const double* part, int m, double* out, cudaStream_t s);
+void vaxpy(double* y, const double* u, double a, int n, cudaStream_t s);   // y += a u
+void vxpby(double* p, const double* z, double b, int n, cudaStream_t s);   // p = z + b p
 void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
                    const double* sc, double* part, cudaStream_t s);
 void pcg_update_p(double* p, const double* z, int n, const double* sc, cudaStream_t s);

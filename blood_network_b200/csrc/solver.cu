@@ -11,12 +11,7 @@
 // interpolation, RAP, symmetrisation, IC(0)); the solve phase uses a
 // multicolour Gauss-Seidel in place of the sequential CF-ordered sweep and a
 // dense direct coarse solve in place of the coarse PCG.
-#include "internal.cuh"
-#include "ichol.cuh"
-#include "dense.cuh"
-#include "solve_kernels.cuh"
-#include "packed.cuh"
-#include "../../include/amg_b200.h"
+#include "solver.cuh"
 
 #include <cub/cub.cuh>
 #include <math.h>
@@ -205,96 +200,6 @@ __global__ void k_to_f32(const double* __restrict__ a, size_t m, T* __restrict__
     b[i] = (T)a[i];
 }
 
-// ------------------------------------------------------------ data
-struct Level {
-  // setup data in the natural numbering (bit-identical to the reference)
-  CSR A, S, P, R;
-  DBuf<int> cf;
-  int n_coarse = 0;
-  int max_lam = 0;
-  // solve phase: the level's unknowns renumbered so that every colour class
-  // is a contiguous range (perm[new] = natural, inv[natural] = new).  Ap is
-  // A renumbered on both sides; Pp maps the next level's numbering into this
-  // one; Rp = Pp^T.  FP32 value copies serve the mixed-precision V-cycle.
-  DBuf<int> perm, inv;
-  CSR Ap, Pp, Rp;
-  RowLayout layA, layP, layR;  // SpMV row-length layouts of Ap, Pp, Rp
-  DBuf<float> A32, P32, R32;
-  // smoother colouring: rows grouped by (set, colour)
-  DBuf<int> gs_rows;
-  std::vector<int> cptr;   // colour class offsets into gs_rows
-  std::vector<char> cjac;  // class is an overflow class (Jacobi update)
-  std::vector<int> clong;  // long rows at the end of each class
-  int colored_for = -1;    // smoother the colouring was built for
-  int color_rounds = 0;
-  int gs_group = 1;        // lanes per row in the GS kernel
-  DBuf<int> d_cptr, d_cjac;  // class tables on the device (single-block sweeps)
-  DBuf<double> l1, dg;
-  DBuf<float> l1_32, dg32;
-  // load-balanced kernels: packings of Ap, Pp, Rp (one range each) and of
-  // the colour classes of Ap (one range per class)
-  Packing pkA, pkP, pkR, pkG;
-  // which operators run on the packed kernels: those with rows longer than
-  // kLongRow (hub rows); the row-group kernels are faster on the others
-  bool use_pkA = false, use_pkP = false, use_pkR = false;
-  // work vectors
-  DBuf<double> b, x, r;
-  DBuf<float> b32, x32, r32;
-};
-
-struct Solver {
-  int device = 0;
-  cudaStream_t s = 0;
-  amg_b200_options opt{};
-  std::vector<std::unique_ptr<Level>> lv;
-  DenseCoarse coarse;
-  CSR Aown;               // solve matrix when set_matrix replaced it
-  CSR Aownp;              // ... renumbered like level 0
-  RowLayout layOwn;
-  bool own_solve = false;
-  DBuf<float> Aown32;
-  IChol ic;
-  bool f32_ready = false;
-  // level-0 preconditioner vectors
-  DBuf<double> u1, r1, icy, icx, xx, r2, corr;
-  DBuf<float> g32, u1f, r1f, icyf, icxf, xxf, r2f, corrf;
-  // PCG vectors
-  DBuf<double> b, x, r, z, p, ap;
-  DBuf<double> sc, part0, part1;
-  double* h_sc = nullptr;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  unsigned long long graph_kernels[2] = {0, 0};
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  amg_solve_stats stats{};
-
-  ~Solver();
-  const CSR& Asolve() const { return own_solve ? Aown : lv[0]->A; }
-  int n() const { return Asolve().n; }
-  void build(CSR&& A0);
-  void rebuild_values(CSR&& A0);
-  void finish_setup();
-  void prepare_f32();
-  void color_level(Level& L, int smoother);
-  void alloc_vectors();
-  void drop_graphs();
-  template <class T> DevMat<T> mat(const CSR& M, const DBuf<float>* v32,
-                                   const RowLayout* lay) const;
-  template <class T> PackedMat<T> pmat(const CSR& M, const DBuf<float>& v32,
-                                       const Packing& pk) const;
-  // V-cycle SpMV and colour classes on the packed kernels (BN_PACKED=0: the
-  // row-group kernels)
-  bool use_packed = getenv("BN_PACKED") == nullptr || atoi(getenv("BN_PACKED")) != 0;
-  const RowLayout& lay_solve() const { return own_solve ? layOwn : lv[0]->layA; }
-  const CSR& Asolve_p() const { return own_solve ? Aownp : lv[0]->Ap; }
-  void build_solve_layout();
-  template <class T> void smooth(int l, const T* bb, T* xl, bool forward);
-  template <class T> void backslash(int l, const T* bb, T* xl);
-  template <class T> void fwdslash(int l, const T* bb, T* xl);
-  template <class T> void precond_t(const T* g, T* out);
-  void precond(const double* g, double* out);  // z = M g (FP64 interface)
-  int pcg(const double* d_b, double* d_x, double tol, int maxiter, int print_level);
-};
-
 Solver::~Solver() {
   drop_graphs();
   if (h_sc) cudaFreeHost(h_sc);
@@ -468,7 +373,7 @@ __global__ void k_iota_perm(int* __restrict__ a, int n) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) a[r] = r;
 }
 
-static void permute_csr(const CSR& A, const int* perm, const int* cinv, CSR& B, cudaStream_t s) {
+void permute_csr(const CSR& A, const int* perm, const int* cinv, CSR& B, cudaStream_t s) {
   const int n = A.n;
   DBuf<int> cnt((size_t)n + 1, s);
   cnt.zero();
@@ -862,6 +767,60 @@ void Solver::precond_t(const T* g, T* out) {
   vadd<T>(XX, CO, n0, out, s);
 }
 
+// amg_vcycle_precond (amg_cycle.c:262-284): x = backslash(g); r = g - A x;
+// x += fwdslash(r), all on the hierarchy's level-0 operator, FP64
+void Solver::vcycle_apply(const double* g, double* out) {
+  const int n0 = lv[0]->A.n;
+  vzero<double>(u1.p, n0, s);
+  backslash<double>(0, g, u1.p);
+  spmv<double>(SPMV_RES, mat<double>(lv[0]->Ap, nullptr, &lv[0]->layA), u1.p, g, r1.p, s);
+  fwdslash<double>(0, r1.p, corr.p);
+  vadd<double>(u1.p, corr.p, n0, out, s);
+}
+
+// amg_backslash (amg_cycle.c:180-215) at level l; x is the initial guess
+void Solver::backslash_at(int l, const double* b, double* x) { backslash<double>(l, b, x); }
+
+// amg_fwdslash (amg_cycle.c:222-253) at level l with x as the initial guess:
+// r = b - A x, coarse correction from R r, x += P e, post-smoothing
+void Solver::fwdslash_at(int l, const double* b, double* x) {
+  const int nl = (int)lv.size();
+  if (l == nl - 1) {
+    coarse.apply<double>(b, x, s);
+    return;
+  }
+  Level& L = *lv[l];
+  Level& C = *lv[l + 1];
+  spmv<double>(SPMV_RES, mat<double>(L.Ap, nullptr, &L.layA), x, b, L.r.p, s);
+  spmv<double>(SPMV_Y, mat<double>(L.Rp, nullptr, &L.layR), L.r.p, nullptr, C.b.p, s);
+  fwdslash<double>(l + 1, C.b.p, C.x.p);
+  spmv<double>(SPMV_ADD, mat<double>(L.Pp, nullptr, &L.layP), C.x.p, nullptr, x, s);
+  smooth<double>(l, b, x, false);
+}
+
+// Solve matrix and IC(0) factor as given (amg_ichol_precond's A and L): the
+// hierarchy stays; A is used as given (no symmetrisation), L as given.
+void Solver::use_matrix_and_factor(CSR* A, CSR&& Lf) {
+  if (A) {
+    Aown = std::move(*A);
+    own_solve = true;
+    permute_csr(Aown, lv[0]->perm.p, lv[0]->inv.p, Aownp, s);
+    analyze_rows(Aownp, layOwn, s);
+  }
+  ic.want_f32 = (opt.precision == AMG_PREC_MIXED);
+  ic.load(std::move(Lf), s);
+  ic.remap(lv[0]->inv.p, s);
+  f32_ready = false;
+  if (opt.precision == AMG_PREC_MIXED) prepare_f32();
+  alloc_vectors();
+  drop_graphs();
+}
+
+void l1_row_norms(const CSR& A, double* d_out, cudaStream_t s) {
+  if (A.n > 0)
+    BN_LAUNCH(k_l1_diag, grid_for(A.n, 256), 256, 0, s, A.ia.p, A.val.p, A.n, d_out);
+}
+
 // z = M r for the PCG: r -> z (captured once per precision as a CUDA graph)
 void Solver::precond(const double* g, double* out) {
   const int mode = opt.precision == AMG_PREC_MIXED ? 1 : 0;
@@ -1014,9 +973,9 @@ static int current_device_count() {
   return c;
 }
 
-// Upload host CSR (validated), symmetrise on the device.
-static void upload_symmetrize(Solver& S, int n, int nnz, const int* ia, const int* ja,
-                              const double* val, bool device_ptrs, CSR& out) {
+// Upload host or device CSR (validated), symmetrise on the device.
+void upload_csr(Solver& S, int n, int nnz, const int* ia, const int* ja, const double* val,
+                bool device_ptrs, bool symmetrise, CSR& out) {
   BN_REQUIRE(n > 0 && nnz >= 0 && ia && ja && val, BN_ERR_ARG, "invalid CSR arguments");
   CSR Ain;
   Ain.alloc(n, n, nnz, S.s, true);
@@ -1028,11 +987,12 @@ static void upload_symmetrize(Solver& S, int n, int nnz, const int* ia, const in
   BN_REQUIRE(!(f & 1), BN_ERR_ARG, "CSR row pointers are not a valid 0-based prefix array");
   BN_REQUIRE(!(f & 2), BN_ERR_ARG, "CSR column index out of range");
   BN_REQUIRE(!(f & 4), BN_ERR_DUP, "CSR row holds a duplicate column index");
-  symmetrize(Ain, out, S.s);
+  if (symmetrise) symmetrize(Ain, out, S.s);
+  else out = std::move(Ain);
 }
 
-static Solver* make_solver(int n, int nnz, const int* ia, const int* ja, const double* val,
-                           const amg_b200_options* o, bool device_ptrs) {
+Solver* make_solver(int n, int nnz, const int* ia, const int* ja, const double* val,
+                    const amg_b200_options* o, bool device_ptrs, bool symmetrise) {
   BN_REQUIRE(current_device_count() > 0, BN_ERR_NO_DEVICE, "no CUDA device available");
   std::unique_ptr<Solver> S(new Solver());
   S->opt = *o;
@@ -1053,23 +1013,11 @@ static Solver* make_solver(int n, int nnz, const int* ia, const int* ja, const d
   BN_CUDA(cudaEventCreate(&S->ev0));
   BN_CUDA(cudaEventCreate(&S->ev1));
   CSR A;
-  upload_symmetrize(*S, n, nnz, ia, ja, val, device_ptrs, A);
+  upload_csr(*S, n, nnz, ia, ja, val, device_ptrs, symmetrise, A);
   S->build(std::move(A));
   return S.release();
 }
 
-template <class F>
-static int guarded(F&& f, int fail) {
-  try {
-    return f();
-  } catch (const Error& e) {
-    set_last_error(e.code, e.what());
-    return fail;
-  } catch (const std::exception& e) {
-    set_last_error(BN_ERR_CUDA, e.what());
-    return fail;
-  }
-}
 
 }  // namespace bn
 
@@ -1133,7 +1081,7 @@ BN_API int amg_solver_update(void* h, int n, int nnz, const int* ia, const int* 
     BN_CUDA(cudaSetDevice(S->device));
     BN_REQUIRE(n == S->lv[0]->A.n, bn::BN_ERR_ARG, "update: dimension differs from the hierarchy");
     bn::CSR A;
-    bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
+    bn::upload_csr(*S, n, nnz, ia, ja, val, false, true, A);
     BN_REQUIRE(A.nnz == S->lv[0]->A.nnz, bn::BN_ERR_ARG, "update: sparsity differs");
     S->rebuild_values(std::move(A));
     bn::set_last_error(0, "");
@@ -1149,7 +1097,7 @@ BN_API int amg_solver_set_matrix(void* h, int n, int nnz, const int* ia, const i
     BN_CUDA(cudaSetDevice(S->device));
     BN_REQUIRE(n == S->lv[0]->A.n, bn::BN_ERR_ARG, "set_matrix: dimension differs");
     bn::CSR A;
-    bn::upload_symmetrize(*S, n, nnz, ia, ja, val, false, A);
+    bn::upload_csr(*S, n, nnz, ia, ja, val, false, true, A);
     S->Aown = std::move(A);
     S->own_solve = true;
     S->ic.want_f32 = (S->opt.precision == AMG_PREC_MIXED);

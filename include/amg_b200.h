@@ -206,6 +206,68 @@ void ichol_compute(const dcsr_mat* A, ichol_factor* L);
 void ichol_solve(const ichol_factor* L, const double* b, double* x);
 void ichol_free(ichol_factor* L);
 
+/* ---------------------------------------------------------------------
+ * The reference's internal hierarchy API (C_amg1/include/amg.h:42-124):
+ * the same struct layout and function signatures, host pointers, backed by
+ * the device solver.  amg_build_hierarchy reads the options from the struct
+ * (threshold, min_size, max_levels, nu, smoother, omega_jacobi, coarsening),
+ * builds the hierarchy on the GPU and fills every level's host fields (A, P,
+ * A_filtered = S, mis, isolated, cf_order, n, n_coarse, l1_diag; the
+ * coarsest level's L_ichol) as the reference does; the device hierarchy is
+ * found again from the amg_data pointer, so the struct must stay at the same
+ * address until amg_free.  Differences: the coarsest level is solved by a
+ * dense FP64 Cholesky (not ichol-PCG to 1e-12) and the smoothers are the
+ * device's multicolour forms.  No struct field is read back after
+ * amg_build_hierarchy: change options through a new build.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  dcsr_mat A;          /* system matrix at this level */
+  dcsr_mat P;          /* prolongation (n_fine x n_coarse) */
+  dcsr_mat A_filtered; /* strength matrix S */
+  int* mis;            /* 1 for a C point, 0 for an F point */
+  int* isolated;       /* all zero */
+  int* cf_order;       /* C points first, then F points */
+  int n;               /* unknowns */
+  int n_coarse;        /* coarse points */
+  ichol_factor L_ichol;/* IC(0) factor of A (coarsest level only) */
+  double* l1_diag;     /* sum_j |a_ij| per row */
+} amg_level;
+
+typedef struct {
+  amg_level levels[AMG_MAX_LEVELS];
+  int num_levels;
+  double threshold;
+  int min_size;
+  int max_levels;
+  int maxit_prol;
+  int lump;
+  int nu;
+  int smoother;
+  double omega_jacobi;
+  int coarsening;
+} amg_data;
+
+/* build_hierarchy.c:29-156, :170-242, :245-260 */
+void amg_build_hierarchy(amg_data* amg, const dcsr_mat* A);
+void amg_rebuild_values(amg_data* amg, const dcsr_mat* A_new);
+void amg_free(amg_data* amg);
+/* amg_cycle.c:214-217, :250-253, :262-284 (x: initial guess for the slashes) */
+void amg_backslash(const amg_data* amg, int lev, const double* b, double* x, int nu);
+void amg_fwdslash(const amg_data* amg, int lev, const double* b, double* x, int nu);
+void amg_vcycle_precond(const amg_data* amg, const double* g, double* x);
+/* amg_ichol_precond.c:51-59.  The first call with a given (A, L) pair loads
+ * them onto the device (A as given; A == &amg->levels[0].A reuses the
+ * hierarchy's); later calls with the same two structs reuse the copies. */
+void amg_ichol_precond(const amg_data* amg, const dcsr_mat* A, const ichol_factor* L,
+                       const double* g, double* x);
+/* amg_pcg.c:12-101: PCG with a host preconditioner callback; A is loaded
+ * onto the device once per call, the vectors live there, and each iteration
+ * hands r to the callback on the host and takes z back.  Returns the
+ * iteration count, or -maxiter without convergence. */
+int amg_pcg(const dcsr_mat* A, const double* b, double* x,
+            void (*precond)(const void* data, const double* g, double* Bg),
+            const void* precond_data, double tol, int maxiter, int print_level);
+
 /* ichol_solve_noalloc: no counterpart in the reference.  Solves L L^T x = b
  * for an IC(0) factor already in device memory (0-based CSR d_ia[n+1],
  * d_ja/d_val[nnz] as ichol_compute returns it, lower triangle, diagonal
