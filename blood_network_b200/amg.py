@@ -140,6 +140,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "amg_ichol_precond": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat),
                                      C.POINTER(IcholFactor), vp, vp]),
         "amg_pcg": (i, [C.POINTER(DcsrMat), vp, vp, PRECOND_FN, vp, d, i, i]),
+        "amg_gauss_seidel_ordered": (i, [i, i, vp, vp, vp, vp, vp, vp, i, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

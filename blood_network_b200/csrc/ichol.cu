@@ -24,6 +24,7 @@
 // their dependencies' values, every wait bounded), or, selectable, as level
 // launches or one cooperative launch with a grid barrier per level.
 #include "ichol.cuh"
+#include "flags.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -396,83 +397,6 @@ k_tri_coop(const int* __restrict__ ia, const int* __restrict__ ja, const T* __re
   }
 }
 
-// Sync-free form: no barrier at all.  Every value of the output vector
-// starts as an all-ones bit pattern (a NaN that arithmetic never produces:
-// results are canonicalised below), so the value itself says whether it has
-// been computed.  A row polls each of its dependencies with relaxed GPU-scope
-// loads until the pattern is gone, then computes and publishes its value
-// with one relaxed store.  Rows are taken in level order, 32 per warp,
-// chunks dealt round-robin to the warps of a co-resident grid: a warp only
-// waits on rows of earlier chunks, and the earliest unfinished chunk has all
-// its dependencies done, so the sweep always advances.  Every wait is
-// bounded; a wait that runs out records an error and uses NaN, so the
-// kernel always ends and the failure surfaces as a non-finite result.
-template <class T>
-struct WordOf;
-template <>
-struct WordOf<float> {
-  using U = unsigned;
-  static constexpr U kPending = 0xFFFFFFFFu;
-  static constexpr U kNaN = 0x7FFFFFFFu;
-};
-template <>
-struct WordOf<double> {
-  using U = unsigned long long;
-  static constexpr U kPending = 0xFFFFFFFFFFFFFFFFull;
-  static constexpr U kNaN = 0x7FFFFFFFFFFFFFFFull;
-};
-
-__device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ float word_value(unsigned u) { return __uint_as_float(u); }
-__device__ __forceinline__ double word_value(unsigned long long u) {
-  return __longlong_as_double((long long)u);
-}
-__device__ __forceinline__ unsigned value_word(float v) { return __float_as_uint(v); }
-__device__ __forceinline__ unsigned long long value_word(double v) {
-  return (unsigned long long)__double_as_longlong(v);
-}
-
-constexpr int kFlagThreads = 256;
-constexpr int kSpinFast = 64;          // polls before backing off
-constexpr int kSpinLimit = 1 << 22;    // polls before giving up (seconds with back-off)
-
-// Waits until none of the first m words u[q] (loaded from o[j[q]]) is
-// pending, re-polling all pending ones together so that the last arrival
-// costs one round trip.
-template <class U>
-__device__ __forceinline__ void wait_group(const U* o, const int (&j)[4], U (&u)[4], int m,
-                                           U pending, U nan, int* err) {
-  for (int it = 0; it < kSpinLimit; it++) {
-    bool pend = false;
-#pragma unroll
-    for (int q = 0; q < 4; q++) pend |= (q < m && u[q] == pending);
-    if (!pend) return;
-    if (it >= kSpinFast) __nanosleep(it < 4096 ? 32 : 256);
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-      if (q < m && u[q] == pending) u[q] = ld_relaxed(o + j[q]);
-  }
-  atomicExch(err, 1);
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-    if (q < m && u[q] == pending) u[q] = nan;
-}
-
 // chunks[c] = [first, end) positions of chunk c: at most 32 rows, never
 // crossing a level boundary, so no lane waits on a lane of its own warp.
 // The warp reconverges after every chunk: lanes of one warp never spin on
@@ -618,23 +542,69 @@ static void make_segments(const std::vector<int>& ptr, std::vector<IChol::Seg>& 
   }
 }
 
-// 32-row chunks of the level-ordered layout, cut at every level boundary
-static int upload_chunks(const std::vector<int>& ptr, DBuf<int2>& d, cudaStream_t s) {
-  std::vector<int2> h;
-  for (size_t l = 0; l + 1 < ptr.size(); l++)
-    for (int t = ptr[l]; t < ptr[l + 1]; t += 32)
-      h.push_back(make_int2(t, t + 32 < ptr[l + 1] ? t + 32 : ptr[l + 1]));
-  d.alloc(h.size() > 0 ? h.size() : 1, s);
-  if (!h.empty()) d.upload(h.data(), h.size());
-  BN_CUDA(cudaStreamSynchronize(s));
-  return (int)h.size();
-}
-
 static void upload_segs(const std::vector<IChol::Seg>& segs, DBuf<int4>& d, cudaStream_t s) {
   std::vector<int4> h(segs.size());
   for (size_t q = 0; q < segs.size(); q++) h[q] = make_int4(segs[q].kind, segs[q].l0, segs[q].l1, 0);
   d.alloc(h.size() > 0 ? h.size() : 1, s);
   if (!h.empty()) d.upload(h.data(), h.size());
+  BN_CUDA(cudaStreamSynchronize(s));
+}
+
+// Dependency levels by a Kahn frontier sweep (level l = rows whose
+// dependencies all lie in levels < l), in one cooperative launch; rows in
+// level order (stable: row order within a level) and the level offsets.
+// deps: row i lists the rows it depends on; users: its transpose.
+void level_schedule(const CSR& deps, const CSR& users, DBuf<int>& order, std::vector<int>& lptr,
+                    cudaStream_t s) {
+  const int n = deps.n;
+  const int g = grid_for(n, 256);
+  DBuf<int> indeg(n, s), level(n, s), frontier(n, s), ctr(1, s);
+  ctr.zero();
+  BN_LAUNCH(k_indeg, g, 256, 0, s, deps.ia.p, n, indeg.p, level.p, frontier.p, ctr.p);
+  int nlevels = 0;
+  {  // all Kahn steps in one cooperative launch
+    DBuf<int> nlev(1, s);
+    int dev = 0, per_sm = 0, sms = 0;
+    BN_CUDA(cudaGetDevice(&dev));
+    BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kahn_all, 256, 0));
+    BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = sms * (per_sm < 4 ? per_sm : 4);
+    BN_REQUIRE(grid > 0, BN_ERR_CUDA, "level sweep grid does not fit");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    g_launch_count++;
+    const int* uia = users.ia.p;
+    const int* uja = users.ja.p;
+    BN_CUDA(cudaLaunchKernelEx(&cfg, k_kahn_all, uia, uja, n, indeg.p, level.p, frontier.p, ctr.p,
+                               nlev.p));
+    const int reached = read_scalar(ctr.p, s);
+    BN_REQUIRE(reached == n, BN_ERR_ARG, "dependency levels did not cover every row");
+    // one step per level; the last one finds no new rows
+    nlevels = read_scalar(nlev.p, s);
+  }
+  order.alloc(n, s);
+  DBuf<int> ids(n, s), keys_out(n, s);
+  BN_LAUNCH(k_iota_i, g, 256, 0, s, ids.p, n);
+  size_t tmp = 0;
+  int eb = 1;
+  while ((1LL << eb) <= (long long)nlevels) eb++;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, level.p, keys_out.p, ids.p, order.p, n, 0,
+                                          eb, s));
+  DBuf<unsigned char> t(tmp, s);
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, level.p, keys_out.p, ids.p, order.p, n, 0, eb,
+                                          s));
+  // level offsets from the sorted levels (every level holds a row)
+  DBuf<int> dptr((size_t)nlevels + 1, s);
+  BN_LAUNCH(k_level_starts, g, 256, 0, s, keys_out.p, n, nlevels, dptr.p);
+  lptr.assign(nlevels + 1, 0);
+  dptr.download(lptr.data(), (size_t)nlevels + 1);
   BN_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -700,57 +670,11 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   }
   offd_nnz = Sl.nnz;
 
-  // Kahn frontier sweep -> level of every row
+  // dependency levels and the level order
   {
     Phase ph("ichol levels", s);
-    DBuf<int> indeg(n, s), level(n, s), frontier(n, s), ctr(1, s);
-    ctr.zero();
-    BN_LAUNCH(k_indeg, g, 256, 0, s, Sl.ia.p, n, indeg.p, level.p, frontier.p, ctr.p);
-    {  // all Kahn steps in one cooperative launch
-      DBuf<int> nlev(1, s);
-      int dev = 0, per_sm = 0, sms = 0;
-      BN_CUDA(cudaGetDevice(&dev));
-      BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kahn_all, 256, 0));
-      BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-      const int grid = sms * (per_sm < 4 ? per_sm : 4);
-      BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): level sweep grid does not fit");
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(grid);
-      cfg.blockDim = dim3(256);
-      cfg.stream = s;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeCooperative;
-      attr[0].val.cooperative = 1;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      g_launch_count++;
-      int* uia = U.ia.p;
-      int* uja = U.ja.p;
-      BN_CUDA(cudaLaunchKernelEx(&cfg, k_kahn_all, (const int*)uia, (const int*)uja, n, indeg.p,
-                                 level.p, frontier.p, ctr.p, nlev.p));
-      const int reached = read_scalar(ctr.p, s);
-      BN_REQUIRE(reached == n, BN_ERR_ARG, "IC(0): dependency levels did not cover every row");
-      // one step per level; the last one finds no new rows
-      nlevels = read_scalar(nlev.p, s);
-    }
-    // level order, stable (natural order within a level)
-    order.alloc(n, s);
-    DBuf<int> ids(n, s), keys_out(n, s);
-    BN_LAUNCH(k_iota_i, g, 256, 0, s, ids.p, n);
-    size_t tmp = 0;
-    int eb = 1;
-    while ((1LL << eb) <= (long long)nlevels) eb++;
-    BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, level.p, keys_out.p, ids.p, order.p, n,
-                                            0, eb, s));
-    DBuf<unsigned char> t(tmp, s);
-    BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, level.p, keys_out.p, ids.p, order.p, n, 0,
-                                            eb, s));
-    // level offsets from the sorted levels (every level holds a row)
-    DBuf<int> dptr((size_t)nlevels + 1, s);
-    BN_LAUNCH(k_level_starts, g, 256, 0, s, keys_out.p, n, nlevels, dptr.p);
-    lptr.assign(nlevels + 1, 0);
-    dptr.download(lptr.data(), (size_t)nlevels + 1);
-    BN_CUDA(cudaStreamSynchronize(s));
+    level_schedule(Sl, U, order, lptr, s);
+    nlevels = (int)lptr.size() - 1;
   }
   // backward processing order: reverse level order
   border.alloc(n, s);

@@ -268,6 +268,20 @@ int amg_pcg(const dcsr_mat* A, const double* b, double* x,
             void (*precond)(const void* data, const double* g, double* Bg),
             const void* precond_data, double tol, int maxiter, int print_level);
 
+/* amg_gauss_seidel_ordered: the computation of the reference's MATLAB
+ * gateway cf_gauss_seidel_mex (Matlab_amg/cf_gauss_seidel_mex.c:27-105), which
+ * has no C-library counterpart: nu Gauss-Seidel sweeps visiting the rows in
+ * `order` (0-based; reversed when backward != 0), x_i = (b_i - sum_{j != i}
+ * a_ij x_j) / d_i with d_i the row's first diagonal entry (1 if none), the
+ * sum in row order, updated values of the rows visited earlier.  Host CSR
+ * and vectors; x holds x0 on entry and the result on exit; bit-identical to
+ * the sequential sweep, computed on the device (rows scheduled by dependency
+ * level).  Returns AMG_OK or a negative AMG_ERR_* code (AMG_ERR_ARG when
+ * order is not a permutation). */
+int amg_gauss_seidel_ordered(int n, int nnz, const int* ia, const int* ja, const double* val,
+                             const double* b, double* x, const int* order, int nu,
+                             int backward);
+
 /* ichol_solve_noalloc: no counterpart in the reference.  Solves L L^T x = b
  * for an IC(0) factor already in device memory (0-based CSR d_ia[n+1],
  * d_ja/d_val[nnz] as ichol_compute returns it, lower triangle, diagonal
