@@ -76,6 +76,13 @@ class AmgData(C.Structure):
                 ("omega_jacobi", C.c_double), ("coarsening", C.c_int)]
 
 
+class NetworkSystem(C.Structure):
+    """amg_network_system: device CSR + rhs of a vessel network's pressure system."""
+    _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("n_nodes", C.c_int),
+                ("ia", C.c_void_p), ("ja", C.c_void_p), ("val", C.c_void_p),
+                ("rhs", C.c_void_p), ("interior_of", C.c_void_p), ("owner", C.c_void_p)]
+
+
 # void (*precond)(const void* data, const double* g, double* Bg)
 PRECOND_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
 
@@ -141,6 +148,12 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                      C.POINTER(IcholFactor), vp, vp]),
         "amg_pcg": (i, [C.POINTER(DcsrMat), vp, vp, PRECOND_FN, vp, d, i, i]),
         "amg_gauss_seidel_ordered": (i, [i, i, vp, vp, vp, vp, vp, vp, i, i]),
+        "amg_network_assemble_device": (i, [i, i, vp, vp, vp, i, vp, vp,
+                                            C.POINTER(NetworkSystem)]),
+        "amg_network_system_free": (None, [C.POINTER(NetworkSystem)]),
+        "amg_network_flows_device": (i, [C.POINTER(NetworkSystem), i, vp, vp, vp, vp, vp]),
+        "amg_network_adjoint_device": (i, [vp, C.POINTER(NetworkSystem), i, vp, vp, vp, vp, d,
+                                           i, vp, vp, ip]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

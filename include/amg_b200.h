@@ -282,6 +282,45 @@ int amg_gauss_seidel_ordered(int n, int nnz, const int* ia, const int* ja, const
                              const double* b, double* x, const int* order, int nu,
                              int backward);
 
+/* ---------------------------------------------------------------------
+ * Vessel networks on the device (device pointers).  The reference assembles
+ * in MATLAB (Matlab_amg/read_nwk.m:17-36, ConnectivityMx.m:10-13); these have
+ * no counterpart in its C library.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  int n;            /* interior unknowns */
+  int nnz;
+  int n_nodes;      /* all nodes */
+  int* ia;          /* device CSR of A = C_I^T G C_I (columns sorted) */
+  int* ja;
+  double* val;
+  double* rhs;      /* device f = -C_I^T G C_B p_B */
+  int* interior_of; /* device: node -> interior unknown, -1 at Dirichlet nodes */
+  void* owner;      /* the library's; release with amg_network_system_free */
+} amg_network_system;
+
+/* Segments u[s] -- v[s] with conductance g[s] between nodes 0..n_nodes-1;
+ * Dirichlet nodes bnd[] (distinct) held at p_bnd[].  Assembles A and f on the
+ * device; entries summed in a fixed order (deterministic). */
+int amg_network_assemble_device(int n_nodes, int n_seg, const int* d_u, const int* d_v,
+                                const double* d_g, int n_bnd, const int* d_bnd,
+                                const double* d_pbnd, amg_network_system* out);
+void amg_network_system_free(amg_network_system* sys);
+/* q[s] = g[s] (P_u - P_v) with P the interior solution p and p_B. */
+int amg_network_flows_device(const amg_network_system* sys, int n_seg, const int* d_u,
+                             const int* d_v, const double* d_g, const double* d_p,
+                             double* d_q);
+/* Adjoint of a loss L(p) through A(g) p = f(g): lambda = A^{-1} dL/dp by
+ * one more solve on `solver` (a handle built for this A; A is symmetric),
+ * then dL/dg[s] = -(Lambda_u - Lambda_v)(P_u - P_v), Lambda = 0 at Dirichlet
+ * nodes.  d_lambda (n) receives lambda.  Returns AMG_OK or a negative
+ * AMG_ERR_*; *iterations (may be NULL) the adjoint solve's count (-maxiter
+ * when it did not converge). */
+int amg_network_adjoint_device(void* solver, const amg_network_system* sys, int n_seg,
+                               const int* d_u, const int* d_v, const double* d_p,
+                               const double* d_dLdp, double tol, int maxiter, double* d_lambda,
+                               double* d_dLdg, int* iterations);
+
 /* ichol_solve_noalloc: no counterpart in the reference.  Solves L L^T x = b
  * for an IC(0) factor already in device memory (0-based CSR d_ia[n+1],
  * d_ja/d_val[nnz] as ichol_compute returns it, lower triangle, diagonal
