@@ -110,6 +110,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "amg_solver_set_stop": (i, [vp, i]),
         "amg_solver_solve": (i, [vp, vp, vp, d, i, i]),
         "amg_solver_solve_device": (i, [vp, vp, vp, d, i, i]),
+        "amg_solver_solve_batch": (i, [vp, i, vp, vp, d, i, vp]),
+        "amg_solver_solve_segmented": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
+        "amg_solver_solve_segmented_device": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
         "amg_solver_precond": (i, [vp, vp, vp]),
         "amg_solver_size": (i, [vp]),
         "amg_solver_num_levels": (i, [vp]),
@@ -234,6 +237,35 @@ class AMGSolver:
         if st not in (0, -4, -5):
             raise AMGError(st, self.lib.amg_solver_last_error().decode())
         return x, it
+
+    def solve_batch(self, B, X0=None, tol=1e-8, maxiter=200):
+        """Columns of the n x k array B, each solved as ``solve`` would;
+        returns (X, iterations per column)."""
+        B = np.asfortranarray(B, dtype=np.float64).reshape(self.n, -1, order="F")
+        k = B.shape[1]
+        X = (np.zeros((self.n, k), order="F") if X0 is None
+             else np.array(X0, dtype=np.float64, order="F", copy=True).reshape(self.n, k, order="F"))
+        its = np.zeros(k, np.int32)
+        rc = self.lib.amg_solver_solve_batch(self.h, k, _p(B), _p(X), tol, maxiter, _p(its))
+        if rc not in (0, -4):
+            raise AMGError(rc, self.lib.amg_solver_last_error().decode())
+        return X, its
+
+    def solve_segmented(self, seg_ptr, b, x0=None, tol=1e-8, maxiter=200):
+        """Block-diagonal independent systems (segment k: rows seg_ptr[k] ..
+        seg_ptr[k+1]-1), each with its own PCG; returns (x, iterations,
+        relres, status) with per-segment iterations and true relative
+        residuals."""
+        ptr = np.ascontiguousarray(seg_ptr, np.int32)
+        nseg = len(ptr) - 1
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        its, rel = np.zeros(nseg, np.int32), np.zeros(nseg)
+        rc = self.lib.amg_solver_solve_segmented(self.h, nseg, _p(ptr), _p(b), _p(x), tol,
+                                                 maxiter, _p(its), _p(rel))
+        if rc not in (0, -4, -5):
+            raise AMGError(rc, self.lib.amg_solver_last_error().decode())
+        return x, its, rel, rc
 
     def precond(self, g):
         g = np.ascontiguousarray(g, dtype=np.float64)

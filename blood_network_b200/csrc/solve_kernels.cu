@@ -559,6 +559,118 @@ void vxpby(double* p, const double* z, double b, int n, cudaStream_t s) {
   if (n > 0) BN_LAUNCH(k_xpby, grid_for(n, 256), 256, 0, s, p, z, b, n);
 }
 
+// ---- segmented PCG (independent systems packed block-diagonally)
+// out[k] = sum over the rows of segment k (natural rows ptr[k]..ptr[k+1]-1,
+// held at solve index idx[row]) of u*v: one block per segment, fixed order
+__global__ void __launch_bounds__(256)
+k_seg_dot(const double* __restrict__ u, const double* __restrict__ v,
+          const int* __restrict__ ptr, const int* __restrict__ idx, int nseg,
+          double* __restrict__ out) {
+  __shared__ double red[32];
+  for (int k = blockIdx.x; k < nseg; k += gridDim.x) {
+    double a = 0.0;
+    for (int r = ptr[k] + threadIdx.x; r < ptr[k + 1]; r += blockDim.x) {
+      const int t = idx[r];
+      a += u[t] * v[t];
+    }
+    const double tot = block_sum(a, red);
+    if (threadIdx.x == 0) out[k] = tot;
+    __syncthreads();
+  }
+}
+void seg_dot(const double* u, const double* v, const int* ptr, const int* idx, int nseg,
+             double* out, cudaStream_t s) {
+  if (nseg > 0) BN_LAUNCH(k_seg_dot, nseg < 4096 ? nseg : 4096, 256, 0, s, u, v, ptr, idx, nseg, out);
+}
+
+// segment of every solve-numbered row: perm[t] is its natural row
+__global__ void k_seg_of_rows(const int* __restrict__ perm, int n, const int* __restrict__ ptr,
+                              int nseg, int* __restrict__ seg) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int r = perm[t];
+    int lo = 0, hi = nseg - 1;  // last segment starting at or before r
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ptr[mid] <= r) lo = mid;
+      else hi = mid - 1;
+    }
+    seg[t] = lo;
+  }
+}
+void seg_of_rows(const int* perm, int n, const int* ptr, int nseg, int* seg, cudaStream_t s) {
+  if (n > 0) BN_LAUNCH(k_seg_of_rows, grid_for(n, 256), 256, 0, s, perm, n, ptr, nseg, seg);
+}
+
+// x += alpha_k p ; r -= alpha_k Ap  (k the row's segment)
+__global__ void k_seg_update_xr(double* __restrict__ x, double* __restrict__ r,
+                                const double* __restrict__ p, const double* __restrict__ ap,
+                                const int* __restrict__ seg, const double* __restrict__ alpha,
+                                int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double a = alpha[seg[i]];
+    x[i] = x[i] + p[i] * a;
+    r[i] = r[i] + ap[i] * (-a);
+  }
+}
+void seg_update_xr(double* x, double* r, const double* p, const double* ap, const int* seg,
+                   const double* alpha, int n, cudaStream_t s) {
+  if (n > 0) BN_LAUNCH(k_seg_update_xr, grid_for(n, 256), 256, 0, s, x, r, p, ap, seg, alpha, n);
+}
+
+// p = z + beta_k p
+__global__ void k_seg_update_p(double* __restrict__ p, const double* __restrict__ z,
+                               const int* __restrict__ seg, const double* __restrict__ beta,
+                               int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = z[i] + p[i] * beta[seg[i]];
+}
+void seg_update_p(double* p, const double* z, const int* seg, const double* beta, int n,
+                  cudaStream_t s) {
+  if (n > 0) BN_LAUNCH(k_seg_update_p, grid_for(n, 256), 256, 0, s, p, z, seg, beta, n);
+}
+
+// per-segment scalars.  sc layout: [SEG_* * nseg + k]
+__global__ void k_seg_alpha(const double* __restrict__ rz, const double* __restrict__ pap,
+                            const int* __restrict__ active, int nseg, double* __restrict__ alpha) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x)
+    alpha[k] = active[k] ? rz[k] / pap[k] : 0.0;
+}
+void seg_alpha(const double* rz, const double* pap, const int* active, int nseg, double* alpha,
+               cudaStream_t s) {
+  if (nseg > 0) BN_LAUNCH(k_seg_alpha, grid_for(nseg, 256), 256, 0, s, rz, pap, active, nseg, alpha);
+}
+
+// beta (standard or flexible), convergence test, rotate rz; counts the
+// segments still iterating into *nactive
+__global__ void k_seg_next(double* __restrict__ rz, const double* __restrict__ rznew,
+                           const double* __restrict__ rzold_new, const double* __restrict__ rr,
+                           const double* __restrict__ bb, const double* __restrict__ rz0,
+                           int* __restrict__ active, int* __restrict__ iters,
+                           double* __restrict__ beta, int nseg, int flexible, int relres,
+                           double tol, int iter, int* nactive) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x) {
+    if (!active[k]) { beta[k] = 0.0; continue; }
+    const double b2 = bb[k] > 0.0 ? bb[k] : 1.0;
+    const double crit = relres ? sqrt(rr[k] / b2) : sqrt(rznew[k] / rz0[k]);
+    beta[k] = flexible ? (rznew[k] - rzold_new[k]) / rz[k] : rznew[k] / rz[k];
+    rz[k] = rznew[k];
+    if (crit < tol || rz0[k] == 0.0 || !isfinite(crit)) {
+      active[k] = 0;
+      iters[k] = isfinite(crit) ? iter : -iter;
+    } else {
+      atomicAdd(nactive, 1);
+    }
+  }
+}
+void seg_next(double* rz, const double* rznew, const double* rzold_new, const double* rr,
+              const double* bb, const double* rz0, int* active, int* iters, double* beta,
+              int nseg, int flexible, int relres, double tol, int iter, int* nactive,
+              cudaStream_t s) {
+  if (nseg > 0)
+    BN_LAUNCH(k_seg_next, grid_for(nseg, 256), 256, 0, s, rz, rznew, rzold_new, rr, bb, rz0,
+              active, iters, beta, nseg, flexible, relres, tol, iter, nactive);
+}
+
 // Reduce a partial array into slot `dst` of the scalar block.
 __global__ void k_reduce(const double* __restrict__ part, int m, double* __restrict__ out) {
   __shared__ double red[32];

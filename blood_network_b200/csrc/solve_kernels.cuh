@@ -97,6 +97,21 @@ void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double*
                   cudaStream_t s);
 void reduce_partials(const double* part, int m, double* out, cudaStream_t s);
 void vaxpy(double* y, const double* u, double a, int n, cudaStream_t s);   // y += a u
+// segmented PCG helpers: segments are natural row ranges ptr[k]..ptr[k+1]-1,
+// idx maps a natural row to its solve index, seg a solve index to its segment
+void seg_dot(const double* u, const double* v, const int* ptr, const int* idx, int nseg,
+             double* out, cudaStream_t s);
+void seg_of_rows(const int* perm, int n, const int* ptr, int nseg, int* seg, cudaStream_t s);
+void seg_update_xr(double* x, double* r, const double* p, const double* ap, const int* seg,
+                   const double* alpha, int n, cudaStream_t s);
+void seg_update_p(double* p, const double* z, const int* seg, const double* beta, int n,
+                  cudaStream_t s);
+void seg_alpha(const double* rz, const double* pap, const int* active, int nseg, double* alpha,
+               cudaStream_t s);
+void seg_next(double* rz, const double* rznew, const double* rzold_new, const double* rr,
+              const double* bb, const double* rz0, int* active, int* iters, double* beta,
+              int nseg, int flexible, int relres, double tol, int iter, int* nactive,
+              cudaStream_t s);
 void vxpby(double* p, const double* z, double b, int n, cudaStream_t s);   // p = z + b p
 void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
                    const double* sc, double* part, cudaStream_t s);

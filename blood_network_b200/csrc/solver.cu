@@ -959,6 +959,130 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   return iter;
 }
 
+// ------------------------------------------------------------ segmented PCG
+namespace {
+// every entry of the solve matrix couples two rows of one segment
+__global__ void k_seg_blockdiag(const int* __restrict__ ia, const int* __restrict__ ja, int n,
+                                const int* __restrict__ seg, int* bad) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int k = seg[t];
+    for (int e = ia[t]; e < ia[t + 1]; e++)
+      if (seg[ja[e]] != k) { atomicExch(bad, 1); break; }
+  }
+}
+// start: a segment iterates unless its r0.z0 is zero (b = A x0 there)
+__global__ void k_seg_start(const double* __restrict__ rz, int nseg, int* __restrict__ active,
+                            int* __restrict__ iters, int* nactive) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x) {
+    const int a = rz[k] != 0.0;
+    active[k] = a;
+    iters[k] = 0;
+    if (a) atomicAdd(nactive, 1);
+  }
+}
+__global__ void k_seg_relres(const double* __restrict__ rr, const double* __restrict__ bb,
+                             int nseg, double* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x)
+    out[k] = sqrt(rr[k]) / (bb[k] > 0.0 ? sqrt(bb[k]) : 1.0);
+}
+}  // namespace
+
+// Independent systems packed block-diagonally (no entry couples two
+// segments), solved together: one SpMV and one preconditioner application a
+// step for all of them, while every segment keeps the scalars, stopping test
+// and iteration count of its own PCG (Solver::pcg applied to that block
+// alone).  The hierarchy of a block-diagonal matrix is block-diagonal (strength,
+// coarsening, interpolation and RAP only follow entries), so the
+// preconditioner acts on every segment separately; a segment that has met its
+// stopping test is frozen (alpha = 0) while the others go on.  Segment dot
+// products are one block per segment over its rows in natural order, so the
+// result does not depend on how the other segments converge.
+int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double* d_x,
+                          double tol, int maxiter, int* h_iters, double* h_relres) {
+  const int n0 = n();
+  const bool flexible = (opt.precision == AMG_PREC_MIXED);
+  if (flexible && !f32_ready) prepare_f32();
+  DevMat<double> A = mat<double>(Asolve_p(), nullptr, &lay_solve());
+  const int* perm0 = lv[0]->perm.p;
+  const int* inv0 = lv[0]->inv.p;
+  DBuf<int> seg(n0, s), ints((size_t)2 * nseg + 2, s);
+  int* active = ints.p;
+  int* iters = ints.p + nseg;
+  int* flag = ints.p + 2 * nseg;  // [0] block-diagonal check, [1] segments iterating
+  ints.zero();
+  seg_of_rows(perm0, n0, d_ptr, nseg, seg.p, s);
+  const CSR& Ap = Asolve_p();
+  BN_LAUNCH(k_seg_blockdiag, grid_for(n0, 256), 256, 0, s, Ap.ia.p, Ap.ja.p, n0, seg.p, flag);
+  BN_REQUIRE(read_scalar(flag, s) == 0, BN_ERR_ARG,
+             "segmented solve: the matrix couples rows of different segments");
+  enum { BB, RR, RZ, RZ0, PAP, RZNEW, RZON, ALPHA, BETA, NSC };
+  DBuf<double> scal((size_t)NSC * nseg, s);
+  auto S_ = [&](int w) { return scal.p + (size_t)w * nseg; };
+  vpermute<double>(d_b, perm0, n0, b.p, false, s);
+  vpermute<double>(d_x, perm0, n0, x.p, false, s);
+  spmv<double>(SPMV_RES, A, x.p, b.p, r.p, s);  // r = b - A x
+  seg_dot(b.p, b.p, d_ptr, inv0, nseg, S_(BB), s);
+  precond(r.p, z.p);
+  BN_CUDA(cudaMemcpyAsync(p.p, z.p, sizeof(double) * n0, cudaMemcpyDeviceToDevice, s));
+  seg_dot(r.p, z.p, d_ptr, inv0, nseg, S_(RZ), s);
+  BN_CUDA(cudaMemcpyAsync(S_(RZ0), S_(RZ), sizeof(double) * nseg, cudaMemcpyDeviceToDevice, s));
+  BN_LAUNCH(k_seg_start, grid_for(nseg, 256), 256, 0, s, S_(RZ), nseg, active, iters, flag + 1);
+  int nact = read_scalar(flag + 1, s);
+  int icerr = ic.take_error(s);
+  if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+  const int relres = (opt.stop == AMG_STOP_RELRES) ? 1 : 0;
+  int iter = 0;
+  for (iter = 1; iter <= maxiter && nact > 0; iter++) {
+    spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s);
+    seg_dot(p.p, ap.p, d_ptr, inv0, nseg, S_(PAP), s);
+    seg_alpha(S_(RZ), S_(PAP), active, nseg, S_(ALPHA), s);
+    seg_update_xr(x.p, r.p, p.p, ap.p, seg.p, S_(ALPHA), n0, s);
+    if (relres) seg_dot(r.p, r.p, d_ptr, inv0, nseg, S_(RR), s);
+    if (flexible) seg_dot(r.p, z.p, d_ptr, inv0, nseg, S_(RZON), s);
+    precond(r.p, z.p);
+    seg_dot(r.p, z.p, d_ptr, inv0, nseg, S_(RZNEW), s);
+    BN_CUDA(cudaMemsetAsync(flag + 1, 0, sizeof(int), s));
+    seg_next(S_(RZ), S_(RZNEW), S_(RZON), S_(RR), S_(BB), S_(RZ0), active, iters, S_(BETA),
+             nseg, flexible ? 1 : 0, relres, tol, iter, flag + 1, s);
+    seg_update_p(p.p, z.p, seg.p, S_(BETA), n0, s);
+    nact = read_scalar(flag + 1, s);
+    icerr = ic.take_error(s);
+    if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+  }
+  // true residual per segment
+  spmv<double>(SPMV_RES, A, x.p, b.p, ap.p, s);
+  seg_dot(ap.p, ap.p, d_ptr, inv0, nseg, S_(RR), s);
+  BN_LAUNCH(k_seg_relres, grid_for(nseg, 256), 256, 0, s, S_(RR), S_(BB), nseg, S_(ALPHA));
+  vpermute<double>(x.p, perm0, n0, d_x, true, s);
+  std::vector<int> hi(2 * (size_t)nseg);
+  std::vector<double> hr(nseg);
+  BN_CUDA(cudaMemcpyAsync(hi.data(), ints.p, sizeof(int) * 2 * nseg, cudaMemcpyDeviceToHost, s));
+  BN_CUDA(cudaMemcpyAsync(hr.data(), S_(ALPHA), sizeof(double) * nseg, cudaMemcpyDeviceToHost, s));
+  BN_CUDA(cudaStreamSynchronize(s));
+  int worst = 0, failed = 0, nan = 0;
+  for (int k = 0; k < nseg; k++) {
+    int it = hi[nseg + k];
+    if (hi[k]) { it = -maxiter; failed = 1; }           // still iterating: no convergence
+    else if (it < 0) nan = 1;                            // stopped on a non-finite value
+    if (h_iters) h_iters[k] = it;
+    if (h_relres) h_relres[k] = hr[k];
+    const int a = it < 0 ? -it : it;
+    if (a > worst) worst = a;
+  }
+  stats.iterations = worst;
+  stats.converged = !(failed || nan);
+  if (nan) {
+    set_last_error(BN_ERR_NAN, "segmented PCG: non-finite value in a segment");
+    return BN_ERR_NAN;
+  }
+  if (failed) {
+    set_last_error(BN_ERR_NOT_CONVERGED, "segmented PCG: a segment did not converge");
+    return BN_ERR_NOT_CONVERGED;
+  }
+  set_last_error(BN_OK, "");
+  return BN_OK;
+}
+
 // ------------------------------------------------------------ host helpers
 static thread_local int t_status = 0;
 static thread_local std::string t_msg;
@@ -1192,6 +1316,79 @@ BN_API int amg_solver_solve(void* h, const double* b, double* x, double tol, int
     return 0;
   }, -1);
   return rc < 0 ? -maxiter : out;
+}
+
+// k right-hand sides on one hierarchy: column j of the column-major n x k
+// arrays B, X is solved as amg_solver_solve would (X holds the initial guesses).
+BN_API int amg_solver_solve_batch(void* h, int k, const double* B, double* X, double tol,
+                                  int maxiter, int* iterations) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_REQUIRE(k >= 0 && (k == 0 || (B && X)), bn::BN_ERR_ARG,
+               "amg_solver_solve_batch: invalid arguments");
+    BN_CUDA(cudaSetDevice(S->device));
+    const size_t n = (size_t)S->n();
+    bn::DBuf<double> db(n * k, S->s), dx(n * k, S->s);
+    db.upload(B, n * k);
+    dx.upload(X, n * k);
+    int failed = 0;
+    for (int j = 0; j < k; j++) {
+      const int it = S->pcg(db.p + n * j, dx.p + n * j, tol, maxiter, 0);
+      if (iterations) iterations[j] = it;
+      failed |= it < 0;
+    }
+    dx.download(X, n * k);
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    if (failed) {
+      bn::set_last_error(bn::BN_ERR_NOT_CONVERGED, "a column did not converge");
+      return (int)bn::BN_ERR_NOT_CONVERGED;
+    }
+    bn::set_last_error(bn::BN_OK, "");
+    return 0;
+  }, bn::BN_ERR_CUDA);
+}
+
+static int solve_segmented(Solver* S, int nseg, const int* seg_ptr, const double* b, double* x,
+                           double tol, int maxiter, int* iterations, double* relres,
+                           bool device) {
+  return bn::guarded([&]() {
+    const int n = S->n();
+    BN_REQUIRE(nseg > 0 && seg_ptr && b && x, bn::BN_ERR_ARG,
+               "segmented solve: invalid arguments");
+    BN_REQUIRE(seg_ptr[0] == 0 && seg_ptr[nseg] == n, bn::BN_ERR_ARG,
+               "segmented solve: segment offsets must run from 0 to n");
+    for (int k = 0; k < nseg; k++)
+      BN_REQUIRE(seg_ptr[k + 1] >= seg_ptr[k], bn::BN_ERR_ARG,
+                 "segmented solve: segment offsets must not decrease");
+    BN_CUDA(cudaSetDevice(S->device));
+    bn::DBuf<int> dptr((size_t)nseg + 1, S->s);
+    dptr.upload(seg_ptr, (size_t)nseg + 1);
+    if (device) return S->pcg_segmented(nseg, dptr.p, b, x, tol, maxiter, iterations, relres);
+    bn::DBuf<double> db(n, S->s), dx(n, S->s);
+    db.upload(b, n);
+    dx.upload(x, n);
+    const int rc = S->pcg_segmented(nseg, dptr.p, db.p, dx.p, tol, maxiter, iterations, relres);
+    dx.download(x, n);
+    BN_CUDA(cudaStreamSynchronize(S->s));
+    return rc;
+  }, bn::BN_ERR_CUDA);
+}
+
+BN_API int amg_solver_solve_segmented(void* h, int nseg, const int* seg_ptr, const double* b,
+                                      double* x, double tol, int maxiter, int* iterations,
+                                      double* relres) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  return solve_segmented((Solver*)h, nseg, seg_ptr, b, x, tol, maxiter, iterations, relres,
+                         false);
+}
+
+BN_API int amg_solver_solve_segmented_device(void* h, int nseg, const int* seg_ptr,
+                                             const double* d_b, double* d_x, double tol,
+                                             int maxiter, int* iterations, double* relres) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  return solve_segmented((Solver*)h, nseg, seg_ptr, d_b, d_x, tol, maxiter, iterations, relres,
+                         true);
 }
 
 BN_API int amg_solver_precond(void* h, const double* g, double* xo) {

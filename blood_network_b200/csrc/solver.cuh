@@ -102,6 +102,10 @@ struct Solver {
   template <class T> void precond_t(const T* g, T* out);
   void precond(const double* g, double* out);  // z = M g (FP64 interface)
   int pcg(const double* d_b, double* d_x, double tol, int maxiter, int print_level);
+  // independent block-diagonal systems (natural row ranges d_ptr[k]..d_ptr[k+1]-1),
+  // each with its own PCG scalars and stopping test; device b, x
+  int pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double* d_x, double tol,
+                    int maxiter, int* h_iters, double* h_relres);
   // FP64 pieces for the reference-named host entry points (device vectors in
   // the solve numbering of the level)
   void vcycle_apply(const double* g, double* out);             // symmetric V-cycle

@@ -242,3 +242,25 @@ def make_config(name: str, seed: int = 0, **kw) -> Network:
     c.pop("coarsening"), c.pop("theta")
     c.update(kw)
     return vascular_network(seed=seed, **c)
+
+
+def block_diagonal(nets):
+    """Independent networks packed into one block-diagonal system (the
+    multi-network batch): returns (n, indptr, indices, data, rhs, seg_ptr),
+    network k holding rows seg_ptr[k] .. seg_ptr[k+1]-1 in its own order."""
+    sizes = np.array([nt.n for nt in nets], np.int64)
+    seg_ptr = np.zeros(len(nets) + 1, np.int64)
+    np.cumsum(sizes, out=seg_ptr[1:])
+    nnzs = np.array([nt.nnz for nt in nets], np.int64)
+    nz_ptr = np.zeros(len(nets) + 1, np.int64)
+    np.cumsum(nnzs, out=nz_ptr[1:])
+    if seg_ptr[-1] > np.iinfo(np.int32).max or nz_ptr[-1] > np.iinfo(np.int32).max:
+        raise ValueError("block_diagonal: the packed system exceeds 32-bit CSR indices")
+    indptr = np.concatenate([[0]] + [nt.indptr[1:].astype(np.int64) + nz_ptr[k]
+                                     for k, nt in enumerate(nets)])
+    indices = np.concatenate([nt.indices.astype(np.int64) + seg_ptr[k]
+                              for k, nt in enumerate(nets)])
+    data = np.concatenate([nt.data for nt in nets])
+    rhs = np.concatenate([nt.rhs for nt in nets])
+    return (int(seg_ptr[-1]), indptr.astype(np.int32), indices.astype(np.int32), data, rhs,
+            seg_ptr.astype(np.int32))

@@ -129,6 +129,31 @@ int amg_solver_set_stop(void* handle, int stop);
 int amg_solver_solve_device(void* handle, const double* d_b, double* d_x, double tol,
                             int maxiter, int print_level);
 
+/* Many right-hand sides on one hierarchy (the batched scenarios of one
+ * network): B and X are column-major n x k host arrays, X holding the initial
+ * guesses; column j is solved exactly as amg_solver_solve would solve it.
+ * iterations[j] (may be NULL) receives that call's return value.  Returns 0,
+ * or AMG_ERR_NOT_CONVERGED (-4) when a column did not converge. */
+int amg_solver_solve_batch(void* handle, int k, const double* B, double* X, double tol,
+                           int maxiter, int* iterations);
+
+/* Independent networks packed block-diagonally into one matrix (no entry
+ * couples two segments; checked, AMG_ERR_ARG otherwise): segment k is the
+ * row range seg_ptr[k] .. seg_ptr[k+1]-1 (host array of nseg + 1 offsets
+ * from 0 to n).  One SpMV and one preconditioner application a step serve
+ * all segments, while each keeps the scalars, stopping test and iteration
+ * count of its own PCG; a converged segment is frozen while the others go
+ * on.  iterations[k] (host, may be NULL): the segment's iteration count, or
+ * -maxiter when it did not converge; relres[k] (may be NULL): its true
+ * ||b - A x|| / ||b||.  Returns 0, AMG_ERR_NOT_CONVERGED (-4) or
+ * AMG_ERR_NAN (-5).  _device: b and x are device pointers. */
+int amg_solver_solve_segmented(void* handle, int nseg, const int* seg_ptr, const double* b,
+                               double* x, double tol, int maxiter, int* iterations,
+                               double* relres);
+int amg_solver_solve_segmented_device(void* handle, int nseg, const int* seg_ptr,
+                                      const double* d_b, double* d_x, double tol, int maxiter,
+                                      int* iterations, double* relres);
+
 /* One application of the AMG+IC(0) preconditioner, x = M g (host arrays),
  * the reference's amg_ichol_precond (C_amg1/src/amg_ichol_precond.c:51). */
 int amg_solver_precond(void* handle, const double* g, double* x);

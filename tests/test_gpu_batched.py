@@ -1,0 +1,117 @@
+"""Batched solves: many right-hand sides on one hierarchy
+(amg_solver_solve_batch), and many independent networks packed
+block-diagonally, each with its own PCG (amg_solver_solve_segmented).
+The segmented PCG's per-segment result is checked against a separate solve of
+that network on its own and against scipy residuals."""
+import numpy as np
+import pytest
+
+from helpers import relres
+from blood_network_b200 import amg
+from blood_network_b200.network import block_diagonal, make_config, vascular_network
+
+
+def _nets():
+    sizes = [(6, 900), (7, 2500), (8, 6000), (6, 1500), (9, 12000)]
+    return [vascular_network(depth=d, n_nodes=m, seed=10 + k) for k, (d, m) in enumerate(sizes)]
+
+
+def test_block_diagonal_layout():
+    nets = _nets()
+    n, ia, ja, val, rhs, ptr = block_diagonal(nets)
+    assert n == sum(nt.n for nt in nets) and ptr[-1] == n and len(ptr) == len(nets) + 1
+    for k, nt in enumerate(nets):
+        r0, r1 = ptr[k], ptr[k + 1]
+        blk = ja[ia[r0]:ia[r1]]
+        assert blk.min() >= r0 and blk.max() < r1
+        assert np.array_equal(val[ia[r0]:ia[r1]], nt.data)
+        assert np.array_equal(rhs[r0:r1], nt.rhs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_batch_columns_equal_single_solves(precision):
+    net = make_config("vascular_20k")
+    rng = np.random.default_rng(3)
+    k = 5
+    B = rng.uniform(0.5, 1.5, (net.n, k)) * net.rhs[:, None]
+    S = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=precision)
+    X, its = S.solve_batch(B, tol=1e-8, maxiter=100)
+    assert X.shape == (net.n, k)
+    for j in range(k):
+        x, it = S.solve(B[:, j].copy(), tol=1e-8, maxiter=100)
+        assert it == its[j] and it > 0
+        assert X[:, j].tobytes() == x.tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_segmented_solves_each_network(precision):
+    nets = _nets()
+    n, ia, ja, val, rhs, ptr = block_diagonal(nets)
+    S = amg.AMGSolver(n, ia, ja, val, precision=precision, stop=amg.STOP_RELRES)
+    tol = 1e-8
+    x, its, rel, rc = S.solve_segmented(ptr, rhs, tol=tol, maxiter=200)
+    assert rc == 0
+    for k, nt in enumerate(nets):
+        r0, r1 = ptr[k], ptr[k + 1]
+        xs = x[r0:r1]
+        got = relres(nt.indptr, nt.indices, nt.data, xs, nt.rhs)
+        assert got < tol and abs(got - rel[k]) <= 1e-3 * tol + 1e-6 * got
+        # the same network solved on its own: same tolerance, similar work
+        Sk = amg.AMGSolver(nt.n, nt.indptr, nt.indices, nt.data, precision=precision,
+                           stop=amg.STOP_RELRES)
+        xk, itk = Sk.solve(nt.rhs, tol=tol, maxiter=200)
+        assert itk > 0 and abs(int(its[k]) - itk) <= max(3, itk // 3)
+        # two solutions of residual < tol differ by up to cond(A) * tol
+        assert np.linalg.norm(xs - xk) <= 1e-4 * np.linalg.norm(xk)
+
+
+@pytest.mark.gpu
+def test_segmented_single_segment_matches_plain_solve():
+    net = make_config("vascular_20k")
+    S = amg.AMGSolver(net.n, net.indptr, net.indices, net.data)
+    x1, it1 = S.solve(net.rhs, tol=1e-8, maxiter=100)
+    x2, its, rel, rc = S.solve_segmented([0, net.n], net.rhs, tol=1e-8, maxiter=100)
+    assert rc == 0 and its[0] == it1
+    assert np.linalg.norm(x2 - x1) <= 1e-9 * np.linalg.norm(x1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_segments_do_not_interact(precision):
+    nets = _nets()[:3]
+    n, ia, ja, val, rhs, ptr = block_diagonal(nets)
+    rhs = rhs.copy()
+    rhs[ptr[1]:ptr[2]] = 0.0  # network 1: b = 0, x0 = 0 -> already solved
+    S = amg.AMGSolver(n, ia, ja, val, precision=precision)
+    x, its, rel, rc = S.solve_segmented(ptr, rhs, tol=1e-8, maxiter=200)
+    assert rc == 0 and its[1] == 0 and not np.any(x[ptr[1]:ptr[2]])
+    assert its[0] > 0 and its[2] > 0
+    # other right-hand sides in networks 1 and 2 (so they iterate and stop
+    # differently) leave network 0's iterates bit for bit as they were
+    rhs2 = rhs.copy()
+    rng = np.random.default_rng(5)
+    rhs2[ptr[1]:] = nets[1].rhs.tolist() + (rng.uniform(0.5, 1.5, ptr[3] - ptr[2])
+                                            * rhs[ptr[2]:]).tolist()
+    x2, its2, _, rc2 = S.solve_segmented(ptr, rhs2, tol=1e-8, maxiter=200)
+    assert rc2 == 0 and its2[1] > 0
+    assert its2[0] == its[0] and x2[:ptr[1]].tobytes() == x[:ptr[1]].tobytes()
+    # and a repeat is deterministic
+    x3, its3, _, _ = S.solve_segmented(ptr, rhs, tol=1e-8, maxiter=200)
+    assert x3.tobytes() == x.tobytes() and np.array_equal(its, its3)
+
+
+@pytest.mark.gpu
+def test_segmented_errors():
+    nets = _nets()[:2]
+    n, ia, ja, val, rhs, ptr = block_diagonal(nets)
+    S = amg.AMGSolver(n, ia, ja, val)
+    with pytest.raises(amg.AMGError):  # splits a connected network
+        S.solve_segmented([0, ptr[1] // 2, n], rhs)
+    with pytest.raises(amg.AMGError):  # offsets do not end at n
+        S.solve_segmented([0, ptr[1]], rhs)
+    with pytest.raises(amg.AMGError):  # decreasing offsets
+        S.solve_segmented([0, ptr[1], ptr[1] - 1, n], rhs)
+    x, its, rel, rc = S.solve_segmented(ptr, rhs, tol=1e-12, maxiter=2)
+    assert rc == -4 and np.all(its == -2)
