@@ -129,6 +129,22 @@ int amg_solver_set_stop(void* handle, int stop);
 int amg_solver_solve_device(void* handle, const double* d_b, double* d_x, double tol,
                             int maxiter, int print_level);
 
+/* ---- Files in the reference's formats (host)
+ * COO text matrix, C_amg1/src/io.c:71-124 (dcsr_mat_dcoo) with the COO -> CSR
+ * conversion of io.c:19-58: header "nrows ncols nnz", then "row col value"
+ * lines; shifted to 0-based when the smallest index is exactly 1; entries of
+ * a row keep their file order and repeated pairs are not summed.  The arrays
+ * are malloc'd: release each with amg_free_host.  AMG_ERR_ARG on a malformed
+ * file or an index out of range (the reference does not check). */
+int amg_read_coo(const char* path, int* nrow, int* ncol, int* nnz, int** ia, int** ja,
+                 double** val);
+void amg_free_host(void* p);
+/* Right-hand side file of C_amg1/test_amg.c:126-148: "n" then n values. */
+int amg_read_vector(const char* path, int n, double* out);
+/* Labelled solution of Matlab_amg/label_solution.m:41-44: "%d %.16e" lines
+ * (1-based node id, pressure). */
+int amg_write_labeled_solution(const char* path, int n, const int* node, const double* p);
+
 /* Many right-hand sides on one hierarchy (the batched scenarios of one
  * network): B and X are column-major n x k host arrays, X holding the initial
  * guesses; column j is solved exactly as amg_solver_solve would solve it.

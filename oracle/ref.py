@@ -336,3 +336,31 @@ def orc_spmv(n, m, A, x, mode="y", b=None, y0=None):
         y = np.zeros(m)
         lib.orc_spmv_t(C.byref(a), _P(x), m, _P(y))
     return y
+
+
+def ref_read_coo(path):
+    """The reference's COO text reader (C_amg1/src/io.c:71-124, compiled from
+    its sources): returns (nrow, ncol, indptr, indices, data) or None when it
+    reports an error."""
+    from blood_network_b200.amg import DcsrMat
+    lib = ref_lib()
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    libc.free.argtypes = [C.c_void_p]
+    lib.dcsr_mat_dcoo.argtypes = [C.c_void_p, C.POINTER(DcsrMat)]
+    lib.dcsr_mat_dcoo.restype = C.c_int
+    fp = libc.fopen(path.encode(), b"r")
+    out = DcsrMat()
+    rc = lib.dcsr_mat_dcoo(fp, C.byref(out))
+    libc.fclose(fp)
+    if rc != 0:
+        return None
+    m, nnz = out.row, out.nnz
+    ia = np.ctypeslib.as_array(out.ia, shape=(m + 1,)).copy()
+    ja = np.ctypeslib.as_array(out.ja, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
+    val = np.ctypeslib.as_array(out.val, shape=(nnz,)).copy() if nnz else np.zeros(0)
+    for p in (out.ia, out.ja, out.val):
+        libc.free(C.cast(p, C.c_void_p))
+    return m, out.col, ia, ja, val
