@@ -35,6 +35,25 @@ namespace bn {
 
 enum : int { kF = -1, kU = 0, kC = 1, kNewC = 2 };
 
+// Points whose S and S^T rows together hold more than kLongPoint entries
+// (hubs of the coarse tree levels, up to ~10^6 entries) are decided by a
+// block each in a second launch of every round; the thread-per-point kernels
+// skip them.  Every rule below is independent of the order in which points
+// are decided within a round, so the split does not change.
+constexpr int kLongPoint = 256;
+constexpr int kLongThreads = 256;
+
+__device__ __forceinline__ bool long_point(const int* __restrict__ sia,
+                                           const int* __restrict__ tia, int i) {
+  return (sia[i + 1] - sia[i]) + (tia[i + 1] - tia[i]) > kLongPoint;
+}
+
+__global__ void k_long_points(const int* __restrict__ sia, const int* __restrict__ tia, int n,
+                              int* __restrict__ list, int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (long_point(sia, tia, i)) list[atomicAdd(counter, 1)] = i;
+}
+
 __global__ void k_lambda(const int* __restrict__ sja, int snnz, int* __restrict__ lam) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < snnz; k += gridDim.x * blockDim.x)
     atomicAdd(&lam[sja[k]], 1);
@@ -57,7 +76,7 @@ __global__ void k_select(const int* __restrict__ sia, const int* __restrict__ sj
                          const double* __restrict__ w, int n, int* cf, int* counter) {
   int local = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (cf[i] != kU) continue;
+    if (cf[i] != kU || long_point(sia, tia, i)) continue;
     const double wi = w[i];
     bool is_max = true;
     for (int k = sia[i]; k < sia[i + 1] && is_max; k++) {
@@ -76,12 +95,39 @@ __global__ void k_select(const int* __restrict__ sia, const int* __restrict__ sj
   if (local) atomicAdd(counter, local);
 }
 
+__global__ void __launch_bounds__(kLongThreads)
+k_select_long(const int* __restrict__ sia, const int* __restrict__ sja,
+              const int* __restrict__ tia, const int* __restrict__ tja,
+              const double* __restrict__ w, const int* __restrict__ list, int m, int* cf,
+              int* counter) {
+  for (int t = blockIdx.x; t < m; t += gridDim.x) {
+    const int i = list[t];
+    if (cf[i] != kU) continue;  // uniform over the block
+    const double wi = w[i];
+    bool beaten = false;
+    for (int k = sia[i] + threadIdx.x; k < sia[i + 1] && !beaten; k += blockDim.x) {
+      const int j = sja[k];
+      beaten = undecided(((volatile int*)cf)[j]) && w[j] > wi;
+    }
+    for (int k = tia[i] + threadIdx.x; k < tia[i + 1] && !beaten; k += blockDim.x) {
+      const int j = tja[k];
+      beaten = undecided(((volatile int*)cf)[j]) && w[j] > wi;
+    }
+    if (!__syncthreads_or(beaten) && threadIdx.x == 0) {
+      cf[i] = kNewC;
+      atomicAdd(counter, 1);
+    }
+    __syncthreads();
+  }
+}
+
 // PMIS mark: new C -> C; undecided with any C in G -> F
 __global__ void k_pmis_mark(const int* __restrict__ sia, const int* __restrict__ sja,
                             const int* __restrict__ tia, const int* __restrict__ tja, int n,
                             int* cf, int* counter) {
   int local = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (long_point(sia, tia, i)) continue;
     int c = cf[i];
     if (c == kNewC) {
       ((volatile int*)cf)[i] = kC;
@@ -105,6 +151,40 @@ __global__ void k_pmis_mark(const int* __restrict__ sia, const int* __restrict__
   if (local) atomicAdd(counter, local);
 }
 
+// mark for the long points (PMIS: S and S^T; RS: S only, new F flagged)
+template <bool PMIS>
+__global__ void __launch_bounds__(kLongThreads)
+k_mark_long(const int* __restrict__ sia, const int* __restrict__ sja,
+            const int* __restrict__ tia, const int* __restrict__ tja,
+            const int* __restrict__ list, int m, int* cf, int* __restrict__ new_f, int* counter) {
+  for (int t = blockIdx.x; t < m; t += gridDim.x) {
+    const int i = list[t];
+    const int c = ((volatile int*)cf)[i];
+    __syncthreads();  // every thread has read cf[i] before thread 0 may change it
+    if (!PMIS && threadIdx.x == 0) new_f[i] = 0;
+    if (c == kNewC) {
+      if (threadIdx.x == 0) ((volatile int*)cf)[i] = kC;
+      continue;
+    }
+    if (c != kU) continue;
+    bool hit = false;
+    for (int k = sia[i] + threadIdx.x; k < sia[i + 1] && !hit; k += blockDim.x) {
+      const int cj = ((volatile int*)cf)[sja[k]];
+      hit = (cj == kC || cj == kNewC);
+    }
+    if (PMIS)
+      for (int k = tia[i] + threadIdx.x; k < tia[i + 1] && !hit; k += blockDim.x) {
+        const int cj = ((volatile int*)cf)[tja[k]];
+        hit = (cj == kC || cj == kNewC);
+      }
+    if (__syncthreads_or(hit) && threadIdx.x == 0) {
+      ((volatile int*)cf)[i] = kF;
+      if (!PMIS) new_f[i] = 1;
+      atomicAdd(counter, 1);
+    }
+  }
+}
+
 __global__ void k_all_undecided_to_c(int n, int* cf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     if (cf[i] == kU || cf[i] == kNewC) cf[i] = kC;
@@ -123,10 +203,12 @@ __global__ void k_rs_measure(const int* __restrict__ lam, int n, double* __restr
 }
 
 // RS mark: new C -> C; undecided i with a (new) C in S_i -> F (flagged new_f)
-__global__ void k_rs_mark(const int* __restrict__ sia, const int* __restrict__ sja, int n, int* cf,
+__global__ void k_rs_mark(const int* __restrict__ sia, const int* __restrict__ sja,
+                          const int* __restrict__ tia, int n, int* cf,
                           int* __restrict__ new_f, int* counter) {
   int local = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (long_point(sia, tia, i)) continue;
     int c = cf[i];
     new_f[i] = 0;
     if (c == kNewC) {
@@ -149,13 +231,29 @@ __global__ void k_rs_mark(const int* __restrict__ sia, const int* __restrict__ s
 }
 
 // each new F raises the measure of its undecided strong dependencies
-__global__ void k_rs_lambda_update(const int* __restrict__ sia, const int* __restrict__ sja, int n,
+// (w stays an integer plus a fixed fraction < 1, so the += 1.0 are exact and
+// their order does not matter)
+__global__ void k_rs_lambda_update(const int* __restrict__ sia, const int* __restrict__ sja,
+                                   const int* __restrict__ tia, int n,
                                    const int* __restrict__ cf, const int* __restrict__ new_f,
                                    double* __restrict__ w) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (!new_f[i]) continue;
+    if (!new_f[i] || long_point(sia, tia, i)) continue;
     for (int k = sia[i]; k < sia[i + 1]; k++) {
       int j = sja[k];
+      if (cf[j] == kU) atomicAdd(&w[j], 1.0);
+    }
+  }
+}
+__global__ void __launch_bounds__(kLongThreads)
+k_rs_lambda_update_long(const int* __restrict__ sia, const int* __restrict__ sja,
+                        const int* __restrict__ list, int m, const int* __restrict__ cf,
+                        const int* __restrict__ new_f, double* __restrict__ w) {
+  for (int t = blockIdx.x; t < m; t += gridDim.x) {
+    const int i = list[t];
+    if (!new_f[i]) continue;
+    for (int k = sia[i] + threadIdx.x; k < sia[i + 1]; k += blockDim.x) {
+      const int j = sja[k];
       if (cf[j] == kU) atomicAdd(&w[j], 1.0);
     }
   }
@@ -219,6 +317,14 @@ __global__ void k_count_c(const int* __restrict__ cf, int n, int* counter) {
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(counter, local);
 }
 
+static void select_round(const CSR& S, const CSR& T, const double* w, int n, int* cf,
+                         const int* longs, int nlong, int glong, int* ctr, cudaStream_t s) {
+  BN_LAUNCH(k_select, grid_for(n, 256), 256, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, w, n, cf, ctr);
+  if (nlong)
+    BN_LAUNCH(k_select_long, glong, kLongThreads, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, w, longs,
+              nlong, cf, ctr);
+}
+
 static void second_pass(const CSR& S, int* cf, cudaStream_t s) {
   const int n = S.n;
   DBuf<int> orphan(n, s), list(n, s), state(n, s), ctr(2, s);
@@ -257,6 +363,16 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
   lam.zero();
   const int g = grid_for(n, 256);
   if (S.nnz > 0) BN_LAUNCH(k_lambda, grid_for(S.nnz, 256), 256, 0, s, S.ja.p, S.nnz, lam.p);
+  DBuf<int> longs;
+  int nlong = 0;
+  {
+    DBuf<int> lst(n, s);
+    ctr.zero();
+    BN_LAUNCH(k_long_points, g, 256, 0, s, S.ia.p, T.ia.p, n, lst.p, ctr.p);
+    nlong = read_scalar(ctr.p, s);
+    if (nlong > 0) longs = std::move(lst);
+  }
+  const int glong = nlong < 4096 ? nlong : 4096;
 
   if (method == COARSEN_PMIS) {
     // rand() sequence after srand(12345), drawn from the host C library
@@ -270,7 +386,7 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
     long long undecided = n;
     for (long long round = 0; undecided > 0 && round <= n; round++) {
       ctr.zero();
-      BN_LAUNCH(k_select, g, 256, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, w.p, n, cf, ctr.p);
+      select_round(S, T, w.p, n, cf, longs.p, nlong, glong, ctr.p, s);
       int nc = read_scalar(ctr.p, s);
       if (nc == 0) {
         BN_LAUNCH(k_all_undecided_to_c, g, 256, 0, s, n, cf);
@@ -278,6 +394,9 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
         break;
       }
       BN_LAUNCH(k_pmis_mark, g, 256, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, n, cf, ctr.p + 1);
+      if (nlong)
+        BN_LAUNCH(k_mark_long<true>, glong, kLongThreads, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p,
+                  longs.p, nlong, cf, (int*)nullptr, ctr.p + 1);
       int nf = read_scalar(ctr.p + 1, s);
       undecided -= (long long)nc + nf;
     }
@@ -292,15 +411,21 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
     long long undecided = n;
     for (long long round = 0; undecided > 0 && round <= n; round++) {
       ctr.zero();
-      BN_LAUNCH(k_select, g, 256, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, w.p, n, cf, ctr.p);
+      select_round(S, T, w.p, n, cf, longs.p, nlong, glong, ctr.p, s);
       int nc = read_scalar(ctr.p, s);
       if (nc == 0) {
         BN_LAUNCH(k_all_undecided_to_c, g, 256, 0, s, n, cf);
         undecided = 0;
         break;
       }
-      BN_LAUNCH(k_rs_mark, g, 256, 0, s, S.ia.p, S.ja.p, n, cf, new_f.p, ctr.p + 1);
-      BN_LAUNCH(k_rs_lambda_update, g, 256, 0, s, S.ia.p, S.ja.p, n, cf, new_f.p, w.p);
+      BN_LAUNCH(k_rs_mark, g, 256, 0, s, S.ia.p, S.ja.p, T.ia.p, n, cf, new_f.p, ctr.p + 1);
+      if (nlong)
+        BN_LAUNCH(k_mark_long<false>, glong, kLongThreads, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p,
+                  longs.p, nlong, cf, new_f.p, ctr.p + 1);
+      BN_LAUNCH(k_rs_lambda_update, g, 256, 0, s, S.ia.p, S.ja.p, T.ia.p, n, cf, new_f.p, w.p);
+      if (nlong)
+        BN_LAUNCH(k_rs_lambda_update_long, glong, kLongThreads, 0, s, S.ia.p, S.ja.p, longs.p,
+                  nlong, cf, new_f.p, w.p);
       int nf = read_scalar(ctr.p + 1, s);
       undecided -= (long long)nc + nf;
     }

@@ -122,6 +122,17 @@ void transpose(const CSR& A, CSR& T, cudaStream_t s, bool with_val) {
 constexpr int kAddCap = 512;   // shared table entries per warp
 constexpr int kAddWarps = 4;   // warps per block
 
+// rows longer than kAddHuge entries of A (coarse-level hubs of up to ~10^6
+// entries): a block per row on the same global table, the misses appended in
+// B's order through a block-wide ballot prefix
+constexpr int kAddHuge = 8192;
+constexpr int kAddBlock = 512;
+
+__device__ __forceinline__ bool add_huge(const int* __restrict__ aia, int i) {
+  return aia[i + 1] - aia[i] > kAddHuge;
+}
+
+
 struct AddTable {
   int* keys;
   int* vals;
@@ -251,6 +262,7 @@ __global__ void k_add_count_g(const int* __restrict__ aia, const int* __restrict
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += warps) {
+    if (add_huge(aia, rows[q])) continue;
     const long long off = toff[q];
     AddTable t{gkeys + off, gvals + off, nullptr, (unsigned)(toff[q + 1] - off) - 1};
     int c = add_count_row(rows[q], t, lane, aia, aja, bia, bja);
@@ -269,10 +281,102 @@ __global__ void k_add_fill_g(const int* __restrict__ aia, const int* __restrict_
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += warps) {
+    if (add_huge(aia, rows[q])) continue;
     const long long off = toff[q];
     AddTable t{gkeys + off, gvals + off, gacc + off / 2, (unsigned)(toff[q + 1] - off) - 1};
     const int i = rows[q];
     add_fill_row(i, t, lane, aia, aja, aval, bia, bja, bval, scale, cia[i], cja, cval);
+  }
+}
+
+__global__ void __launch_bounds__(kAddBlock)
+k_add_count_b(const int* __restrict__ aia, const int* __restrict__ aja,
+              const int* __restrict__ bia, const int* __restrict__ bja,
+              const int* __restrict__ rows, int m, const long long* __restrict__ toff,
+              int* __restrict__ gkeys, int* __restrict__ gvals, int* __restrict__ cnt) {
+  __shared__ int red[kAddBlock / 32];
+  for (int q = blockIdx.x; q < m; q += gridDim.x) {
+    const int i = rows[q];
+    if (!add_huge(aia, i)) continue;
+    const long long off = toff[q];
+    AddTable t{gkeys + off, gvals + off, nullptr, (unsigned)(toff[q + 1] - off) - 1};
+    const int a0 = aia[i], la = aia[i + 1] - a0;
+    const int b0 = bia[i], lb = bia[i + 1] - b0;
+    for (unsigned e = threadIdx.x; e <= t.mask; e += blockDim.x) t.keys[e] = -1;
+    __syncthreads();
+    for (int k = threadIdx.x; k < la; k += blockDim.x) tbl_insert(t, aja[a0 + k], k);
+    __syncthreads();
+    int extra = 0;
+    for (int k = threadIdx.x; k < lb; k += blockDim.x) extra += (tbl_find(t, bja[b0 + k]) < 0);
+    for (int o = 16; o > 0; o >>= 1) extra += __shfl_xor_sync(0xffffffffu, extra, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = extra;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = la;
+      for (int w = 0; w < kAddBlock / 32; w++) tot += red[w];
+      cnt[i] = tot;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kAddBlock)
+k_add_fill_b(const int* __restrict__ aia, const int* __restrict__ aja,
+             const double* __restrict__ aval, const int* __restrict__ bia,
+             const int* __restrict__ bja, const double* __restrict__ bval,
+             const int* __restrict__ rows, int m, double scale,
+             const long long* __restrict__ toff, int* __restrict__ gkeys,
+             int* __restrict__ gvals, double* __restrict__ gacc, const int* __restrict__ cia,
+             int* __restrict__ cja, double* __restrict__ cval) {
+  __shared__ int wmiss[kAddBlock / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int q = blockIdx.x; q < m; q += gridDim.x) {
+    const int i = rows[q];
+    if (!add_huge(aia, i)) continue;
+    const long long off = toff[q];
+    AddTable t{gkeys + off, gvals + off, gacc + off / 2, (unsigned)(toff[q + 1] - off) - 1};
+    const int a0 = aia[i], la = aia[i + 1] - a0;
+    const int b0 = bia[i], lb = bia[i + 1] - b0;
+    const int p0 = cia[i];
+    for (unsigned e = threadIdx.x; e <= t.mask; e += blockDim.x) t.keys[e] = -1;
+    __syncthreads();
+    for (int k = threadIdx.x; k < la; k += blockDim.x) {
+      const int c = aja[a0 + k];
+      tbl_insert(t, c, k);
+      t.acc[k] = aval[a0 + k];
+      cja[p0 + k] = c;
+    }
+    __syncthreads();
+    int appended = 0;
+    for (int base = 0; base < lb; base += blockDim.x) {
+      const int k = base + threadIdx.x;
+      int pos = -2, c = 0;
+      double v = 0.0;
+      if (k < lb) {
+        c = bja[b0 + k];
+        v = bval[b0 + k];
+        pos = tbl_find(t, c);
+        if (pos >= 0) t.acc[pos] = xadd(t.acc[pos], v);  // one writer per slot
+      }
+      const unsigned miss = __ballot_sync(0xffffffffu, pos == -1);
+      if (lane == 0) wmiss[w] = __popc(miss);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int u = 0; u < kAddBlock / 32; u++) {
+        before += (u < w) ? wmiss[u] : 0;
+        total += wmiss[u];
+      }
+      if (pos == -1) {
+        const int o = p0 + la + appended + before + __popc(miss & lt);
+        cja[o] = c;
+        cval[o] = xmul(v, scale);
+      }
+      appended += total;
+      __syncthreads();
+    }
+    for (int k = threadIdx.x; k < la; k += blockDim.x) cval[p0 + k] = xmul(t.acc[k], scale);
+    __syncthreads();
   }
 }
 
@@ -313,6 +417,8 @@ void add_scaled(const CSR& A, const CSR& B, double scale, CSR& C, cudaStream_t s
     gacc.alloc((size_t)total / 2 + 1, s);
     BN_LAUNCH(k_add_count_g, gl, 128, 0, s, A.ia.p, A.ja.p, B.ia.p, B.ja.p, lrows.p, m, toff.p,
               gkeys.p, gvals.p, cnt.p);
+    BN_LAUNCH(k_add_count_b, m < 1024 ? m : 1024, kAddBlock, 0, s, A.ia.p, A.ja.p, B.ia.p,
+              B.ja.p, lrows.p, m, toff.p, gkeys.p, gvals.p, cnt.p);
   }
   int nnz = scan_counts(cnt.p, n, s);
   C.n = n; C.m = A.m; C.nnz = nnz;
@@ -322,9 +428,13 @@ void add_scaled(const CSR& A, const CSR& B, double scale, CSR& C, cudaStream_t s
   if (n > 0)
     BN_LAUNCH(k_add_fill_w, gw, 32 * kAddWarps, 0, s, A.ia.p, A.ja.p, A.val.p, B.ia.p, B.ja.p,
               B.val.p, n, scale, C.ia.p, C.ja.p, C.val.p);
-  if (m > 0)
+  if (m > 0) {
     BN_LAUNCH(k_add_fill_g, gl, 128, 0, s, A.ia.p, A.ja.p, A.val.p, B.ia.p, B.ja.p, B.val.p,
               lrows.p, m, scale, toff.p, gkeys.p, gvals.p, gacc.p, C.ia.p, C.ja.p, C.val.p);
+    BN_LAUNCH(k_add_fill_b, m < 1024 ? m : 1024, kAddBlock, 0, s, A.ia.p, A.ja.p, A.val.p,
+              B.ia.p, B.ja.p, B.val.p, lrows.p, m, scale, toff.p, gkeys.p, gvals.p, gacc.p,
+              C.ia.p, C.ja.p, C.val.p);
+  }
 }
 
 void symmetrize(const CSR& A, CSR& out, cudaStream_t s) {

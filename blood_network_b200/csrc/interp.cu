@@ -128,6 +128,163 @@ __device__ __forceinline__ int hub_find(const int* __restrict__ keys, const int*
   }
 }
 
+// F rows with more than kWarpRow entries of A (and at most kInterpMaxC
+// strong points) are evaluated by a warp.  The operations and their order
+// are those of the thread-per-row kernel: the lanes classify A's entries and
+// locate the strong C points, one lane adds the weak entries in row order,
+// the strong F neighbours are taken from S_i (the same entries of A in the
+// same order, S holding A's values), the entries of each neighbour's row
+// that lie in C_i are collected in row order and one lane sums the
+// denominator in that order; each slot of P's row receives its terms in the
+// same sequence as in the thread kernel.
+constexpr int kWarpRow = 32;
+
+__device__ __forceinline__ bool warp_row(const int* __restrict__ aia, const int* __restrict__ sia,
+                                         int i) {
+  return aia[i + 1] - aia[i] > kWarpRow && sia[i + 1] - sia[i] <= kInterpMaxC;
+}
+
+__global__ void k_warp_rows(const int* __restrict__ aia, const int* __restrict__ sia,
+                            const int* __restrict__ cf, int n, int* __restrict__ list,
+                            int* counter) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (cf[i] != 1 && warp_row(aia, sia, i)) list[atomicAdd(counter, 1)] = i;
+}
+
+constexpr int kInterpWarps = 4;
+
+__global__ void __launch_bounds__(32 * kInterpWarps)
+k_interp_values_warp(const int* __restrict__ aia, const int* __restrict__ aja,
+                     const double* __restrict__ aval, const int* __restrict__ sia,
+                     const int* __restrict__ sja, const double* __restrict__ sval,
+                     const int* __restrict__ cf, const int* __restrict__ rows, int m,
+                     const int* __restrict__ pia, double* __restrict__ pval,
+                     const int* __restrict__ hubidx, const int* __restrict__ hoff,
+                     const int* __restrict__ hkeys, const int* __restrict__ hvals) {
+  __shared__ int s_col[kInterpWarps][32];   // S_i columns, S order
+  __shared__ int s_slot[kInterpWarps][32];  // slot in P's row (C) or -1 (F)
+  __shared__ int s_cm[kInterpWarps][32];    // C_i columns by slot
+  __shared__ double s_buf[kInterpWarps][32];
+  __shared__ int s_el[kInterpWarps][32], s_sl[kInterpWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* col = s_col[w];
+  int* slt = s_slot[w];
+  int* cm = s_cm[w];
+  double* buf = s_buf[w];
+  int* el = s_el[w];
+  int* sl = s_sl[w];
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m; r += warps) {
+    const int i = rows[r];
+    const int p0 = pia[i];
+    const int s0 = sia[i], ns = sia[i + 1] - s0;
+    // strong points of i and their slots
+    int q = -1, isc = 0;
+    if (lane < ns) {
+      q = sja[s0 + lane];
+      isc = (cf[q] == 1);
+    }
+    const unsigned cmask = __ballot_sync(0xffffffffu, isc);
+    const int nc = __popc(cmask);
+    if (lane < ns) {
+      col[lane] = q;
+      slt[lane] = isc ? __popc(cmask & lt) : -1;
+      if (isc) cm[__popc(cmask & lt)] = q;
+    }
+    if (lane < nc) pval[p0 + lane] = 0.0;
+    __syncwarp();
+    // A_i: diagonal, direct C terms, weak sum (one lane, row order)
+    double diag = 0.0, weak = 0.0;
+    const int a0 = aia[i], a1 = aia[i + 1];
+    for (int base = a0; base < a1; base += 32) {
+      const int k = base + lane;
+      int cls = 0;  // 0 none, 1 weak, 2 diagonal
+      double a = 0.0;
+      if (k < a1) {
+        const int j = aja[k];
+        a = aval[k];
+        if (j == i) {
+          cls = 2;
+        } else {
+          int at = -1;
+          for (int t = 0; t < ns; t++)
+            if (col[t] == j) { at = t; break; }
+          if (at < 0) cls = 1;
+          else if (slt[at] >= 0) pval[p0 + slt[at]] = xadd(pval[p0 + slt[at]], a);  // once per slot
+        }
+      }
+      const unsigned wm = __ballot_sync(0xffffffffu, cls == 1);
+      if (cls == 1) buf[__popc(wm & lt)] = a;
+      const unsigned dm = __ballot_sync(0xffffffffu, cls == 2);
+      if (dm) diag = __shfl_sync(0xffffffffu, a, __ffs(dm) - 1);
+      __syncwarp();
+      if (lane == 0) {
+        const int nw = __popc(wm);
+        for (int t = 0; t < nw; t++) weak = xadd(weak, buf[t]);
+      }
+      __syncwarp();
+    }
+    double diag_hat = xadd(diag, weak);  // meaningful on lane 0
+    // strong F neighbours in S order (= A order)
+    for (int t = 0; t < ns; t++) {
+      if (slt[t] >= 0) continue;
+      const int kk = col[t];
+      const double a_ik = sval[s0 + t];
+      const int h = hubidx ? hubidx[kk] : -1;
+      int ne = 0;
+      if (h >= 0) {
+        // entries of the hub row in C_i by lookup, then ranked by position
+        const int l = lane < nc ? hub_find(hkeys, hvals, hoff, h, cm[lane]) : -1;
+        const unsigned fm = __ballot_sync(0xffffffffu, l >= 0);
+        ne = __popc(fm);
+        int rank = 0;
+        for (int u = 0; u < 32; u++) {
+          const int lu = __shfl_sync(0xffffffffu, l, u);
+          rank += (lu >= 0 && l >= 0 && lu < l);
+        }
+        if (l >= 0) {
+          el[rank] = l;
+          sl[rank] = lane;
+        }
+      } else {
+        for (int base = aia[kk]; base < aia[kk + 1]; base += 32) {
+          const int l = base + lane;
+          int sidx = -1;
+          if (l < aia[kk + 1]) {
+            const int mcol = aja[l];
+            if (cf[mcol] == 1)
+              for (int u = 0; u < nc; u++)
+                if (cm[u] == mcol) { sidx = u; break; }
+          }
+          const unsigned fm = __ballot_sync(0xffffffffu, sidx >= 0);
+          if (sidx >= 0) {
+            const int o = ne + __popc(fm & lt);
+            el[o] = l;
+            sl[o] = sidx;
+          }
+          ne += __popc(fm);
+        }
+      }
+      __syncwarp();
+      double denom = 0.0;
+      if (lane == 0)
+        for (int u = 0; u < ne; u++) denom = xadd(denom, aval[el[u]]);
+      denom = __shfl_sync(0xffffffffu, denom, 0);
+      if (fabs(denom) < 1e-15) {
+        if (lane == 0) diag_hat = xadd(diag_hat, a_ik);
+      } else if (lane < ne) {
+        const int o = p0 + sl[lane];
+        pval[o] = xadd(pval[o], xdiv(xmul(a_ik, aval[el[lane]]), denom));
+      }
+      __syncwarp();
+    }
+    diag_hat = __shfl_sync(0xffffffffu, diag_hat, 0);
+    if (fabs(diag_hat) > 1e-15 && lane < nc) pval[p0 + lane] = xdiv(pval[p0 + lane], -diag_hat);
+    __syncwarp();
+  }
+}
+
 __global__ void k_interp_values(const int* __restrict__ aia, const int* __restrict__ aja,
                                 const double* __restrict__ aval, const int* __restrict__ sia,
                                 const int* __restrict__ sja, const int* __restrict__ cf, int n,
@@ -140,6 +297,7 @@ __global__ void k_interp_values(const int* __restrict__ aia, const int* __restri
       pval[p0] = 1.0;
       continue;
     }
+    if (warp_row(aia, sia, i)) continue;  // k_interp_values_warp
     const int s0 = sia[i], s1 = sia[i + 1];
     for (int p = p0; p < p1; p++) pval[p] = 0.0;
     double diag = 0.0, weak = 0.0;
@@ -253,6 +411,14 @@ void interpolation_values(const CSR& A, const CSR& S, const int* cf, CSR& P, cud
   BN_LAUNCH(k_interp_values, grid_for(n, 128), 128, 0, s, A.ia.p, A.ja.p, A.val.p, S.ia.p,
             S.ja.p, cf, n, P.ia.p, P.val.p, nh > 0 ? hubidx.p : nullptr, hoff.p, keys.p,
             vals.p);
+  ctr.zero();
+  BN_LAUNCH(k_warp_rows, grid_for(n, 256), 256, 0, s, A.ia.p, S.ia.p, cf, n, hubrows.p, ctr.p);
+  const int nw = read_scalar(ctr.p, s);
+  if (nw > 0)
+    BN_LAUNCH(k_interp_values_warp, grid_for((long long)nw * 32, 32 * kInterpWarps, 8),
+              32 * kInterpWarps, 0, s, A.ia.p, A.ja.p, A.val.p, S.ia.p, S.ja.p, S.val.p, cf,
+              hubrows.p, nw, P.ia.p, P.val.p, nh > 0 ? hubidx.p : nullptr, hoff.p, keys.p,
+              vals.p);
 }
 
 void interpolation_pattern(const CSR& S, const int* cf, int n_coarse, CSR& P, cudaStream_t s) {
