@@ -141,6 +141,7 @@ __device__ int rap_count_row(int ic, Table t, int lane, const int* __restrict__ 
   return cnt;
 }
 
+template <int BUF = kBuf>
 __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
                              const int* __restrict__ ria, const int* __restrict__ rja,
                              const double* __restrict__ rval, const int* __restrict__ aia,
@@ -182,17 +183,17 @@ __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
       const int total = __shfl_sync(0xffffffffu, incl, 31);
       const int start = incl - plen;
       (void)lt;
-      for (int cs = 0; cs < total; cs += kBuf) {
+      for (int cs = 0; cs < total; cs += BUF) {
         for (int q = 0; q < plen; q++) {
           const int sidx = start + q - cs;
-          if (sidx >= 0 && sidx < kBuf) {
+          if (sidx >= 0 && sidx < BUF) {
             bcol[sidx] = pja[p0 + q];
             bval[sidx] = xmul(ra, pval[p0 + q]);
           }
         }
         __syncwarp();
         if (lane == 0) {
-          const int m = min(kBuf, total - cs);
+          const int m = min(BUF, total - cs);
           for (int q = 0; q < m; q++) {
             const int col = bcol[q];
             const double v = bval[q];
@@ -214,6 +215,49 @@ __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
   nslots = __shfl_sync(0xffffffffu, nslots, 0);
   for (int q = lane; q < nslots; q += 32) cval[cbase + q] = t.vals[q];
   __syncwarp();
+}
+
+// ---------------- small rows (at most kSmallCap/2 products): small tables
+// and stream buffers, so that many more warps per SM hide the latency of the
+// R -> A -> P walk (the fine and first coarse levels are almost all small)
+constexpr int kSmallCap = 128;
+constexpr int kSmallBuf = 64;
+constexpr int kSmallWarps = 8;
+
+__global__ void __launch_bounds__(32 * kSmallWarps)
+k_rap_count_small(const int* __restrict__ ria, const int* __restrict__ rja,
+                  const int* __restrict__ aia, const int* __restrict__ aja,
+                  const int* __restrict__ pia, const int* __restrict__ pja,
+                  const int* __restrict__ rows, int m, int* __restrict__ cnt_out) {
+  __shared__ int keys_s[kSmallWarps][kSmallCap];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Table t{keys_s[w], nullptr, nullptr, kSmallCap - 1};
+  for (int q = blockIdx.x * kSmallWarps + w; q < m; q += gridDim.x * kSmallWarps) {
+    const int ic = rows[q];
+    int c = rap_count_row(ic, t, lane, ria, rja, aia, aja, pia, pja);
+    if (lane == 0) cnt_out[ic] = c;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kSmallWarps)
+k_rap_fill_small(const int* __restrict__ ria, const int* __restrict__ rja,
+                 const double* __restrict__ rval, const int* __restrict__ aia,
+                 const int* __restrict__ aja, const double* __restrict__ aval,
+                 const int* __restrict__ pia, const int* __restrict__ pja,
+                 const double* __restrict__ pval, const int* __restrict__ rows, int m,
+                 const int* __restrict__ cia, int* __restrict__ cja, double* __restrict__ cval) {
+  __shared__ double vals_s[kSmallWarps][kSmallCap / 2];
+  __shared__ double bval_s[kSmallWarps][kSmallBuf];
+  __shared__ int keys_s[kSmallWarps][kSmallCap];
+  __shared__ int slots_s[kSmallWarps][kSmallCap];
+  __shared__ int bcol_s[kSmallWarps][kSmallBuf];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Table t{keys_s[w], slots_s[w], vals_s[w], kSmallCap - 1};
+  for (int q = blockIdx.x * kSmallWarps + w; q < m; q += gridDim.x * kSmallWarps) {
+    const int ic = rows[q];
+    rap_fill_row<kSmallBuf>(ic, t, lane, bcol_s[w], bval_s[w], ria, rja, rval, aia, aja, aval,
+                            pia, pja, pval, cia[ic], cja, cval);
+  }
 }
 
 // ---------------- pass 1 kernels
@@ -745,14 +789,15 @@ static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
 }
 
 // ---------------- classification helpers
-// class by a size estimate: 0 (<= kWarpCap/2), 1 (<= kBigCap/2), 2 (beyond)
+// class by a size estimate: 3 (<= kSmallCap/2), 0 (<= kWarpCap/2),
+// 1 (<= kBigCap/2), 2 (beyond)
 __global__ void k_rap_classify(const long long* __restrict__ est, int nc, int cap_limit,
                                int* __restrict__ lists, int* __restrict__ counts) {
   for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
     long long e = est[ic];
     if (e < 0) continue;  // handled elsewhere
     if (e > cap_limit) e = cap_limit;
-    int c = e <= kWarpCap / 2 ? 0 : (e <= kBigCap / 2 ? 1 : 2);
+    int c = e <= kSmallCap / 2 ? 3 : (e <= kWarpCap / 2 ? 0 : (e <= kBigCap / 2 ? 1 : 2));
     int pos = atomicAdd(&counts[c], 1);
     lists[(size_t)c * nc + pos] = ic;
   }
@@ -789,17 +834,17 @@ __global__ void k_i32_to_i64(const int* __restrict__ a, int n, long long* __rest
 }
 
 struct RapClasses {
-  DBuf<int> lists;  // 3 x nc
-  int count[3] = {0, 0, 0};
+  DBuf<int> lists;  // 4 x nc
+  int count[4] = {0, 0, 0, 0};
 };
 
 static void classify(const long long* est, int nc, RapClasses& rc, cudaStream_t s) {
-  rc.lists.alloc((size_t)3 * (nc > 0 ? nc : 1), s);
-  DBuf<int> cnt(3, s);
+  rc.lists.alloc((size_t)4 * (nc > 0 ? nc : 1), s);
+  DBuf<int> cnt(4, s);
   cnt.zero();
   if (nc > 0)
     BN_LAUNCH(k_rap_classify, grid_for(nc, 256), 256, 0, s, est, nc, nc, rc.lists.p, cnt.p);
-  cnt.download(rc.count, 3);
+  cnt.download(rc.count, 4);
   BN_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -848,7 +893,11 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
     const int* L0 = rc.lists.p;
     const int* L1 = rc.lists.p + nc;
     const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    const int* L3 = rc.lists.p + 3 * (size_t)nc;
     Phase ph("rap count", s);
+    if (rc.count[3])
+      BN_LAUNCH(k_rap_count_small, grid_for(rc.count[3], kSmallWarps, 64), 32 * kSmallWarps, 0,
+                s, R.ia.p, R.ja.p, A.ia.p, A.ja.p, P.ia.p, P.ja.p, L3, rc.count[3], cnt.p);
     if (rc.count[0])
       BN_LAUNCH(k_rap_count_warp, grid_for(rc.count[0], kRapWarps, 64), 32 * kRapWarps, 0, s,
                 R.ia.p, R.ja.p, A.ia.p, A.ja.p, P.ia.p, P.ja.p, L0, rc.count[0], cnt.p);
@@ -891,10 +940,15 @@ void rap(const CSR& R, const CSR& A, const CSR& P, CSR& Ac, cudaStream_t s) {
     const int* L0 = rc.lists.p;
     const int* L1 = rc.lists.p + nc;
     const int* L2 = rc.lists.p + 2 * (size_t)nc;
+    const int* L3 = rc.lists.p + 3 * (size_t)nc;
     if (trace_on())
-      fprintf(stderr, "[bn]     rap fill classes: warp %d big %d huge %d hubs %d\n", rc.count[0],
-              rc.count[1], rc.count[2], nhub);
+      fprintf(stderr, "[bn]     rap fill classes: small %d warp %d big %d huge %d hubs %d\n",
+              rc.count[3], rc.count[0], rc.count[1], rc.count[2], nhub);
     Phase ph_w("rap fill warp", s);
+    if (rc.count[3])
+      BN_LAUNCH(k_rap_fill_small, grid_for(rc.count[3], kSmallWarps, 64), 32 * kSmallWarps, 0, s,
+                R.ia.p, R.ja.p, R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p, P.ja.p, P.val.p, L3,
+                rc.count[3], Ac.ia.p, Ac.ja.p, Ac.val.p);
     if (rc.count[0])
       BN_LAUNCH(k_rap_fill_warp, grid_for(rc.count[0], kRapWarps, 32), 32 * kRapWarps,
                 kWarpFillSmem, s, R.ia.p, R.ja.p, R.val.p, A.ia.p, A.ja.p, A.val.p, P.ia.p,

@@ -41,6 +41,7 @@ constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 
 constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than this are capped
 constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
+constexpr int kColorHuge = 4096;    // ... and longer than this by a block
 constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
@@ -88,7 +89,7 @@ __global__ void k_color_round_long(const int* __restrict__ ia, const int* __rest
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nl; w += warps) {
     const int i = lrows[w];
-    if (color[i] >= 0) continue;
+    if (color[i] >= 0 || ia[i + 1] - ia[i] > kColorHuge) continue;
     const unsigned long long pi =
         ((unsigned long long)(ia[i + 1] - ia[i]) << 32) | color_hash((unsigned)i);
     const int si = set ? set[i] : 0;
@@ -117,6 +118,54 @@ __global__ void k_color_round_long(const int* __restrict__ ia, const int* __rest
       newc[i] = c < cap ? c : kMaxColors;
       atomicAdd(counter, 1);
     }
+  }
+}
+
+// rows longer than kColorHuge (coarse-level hubs): a block per row, the
+// same decision as the warp kernel
+__global__ void __launch_bounds__(512)
+k_color_round_huge(const int* __restrict__ ia, const int* __restrict__ ja,
+                   const int* __restrict__ set, const int* __restrict__ lrows, int nl,
+                   const int* __restrict__ color, int* __restrict__ newc, int* counter, int cap) {
+  __shared__ unsigned s_used;
+  for (int w = blockIdx.x; w < nl; w += gridDim.x) {
+    const int i = lrows[w];
+    if (color[i] >= 0 || ia[i + 1] - ia[i] <= kColorHuge) continue;  // uniform
+    const unsigned long long pi =
+        ((unsigned long long)(ia[i + 1] - ia[i]) << 32) | color_hash((unsigned)i);
+    const int si = set ? set[i] : 0;
+    if (threadIdx.x == 0) s_used = 0;
+    __syncthreads();
+    unsigned used = 0;
+    bool blocked = false;
+    for (int k0 = ia[i]; k0 < ia[i + 1]; k0 += blockDim.x) {
+      const int k = k0 + threadIdx.x;
+      if (k < ia[i + 1]) {
+        const int j = ja[k];
+        if (j != i && !(set && set[j] != si)) {
+          const int cj = color[j];
+          if (cj >= 0) {
+            if (cj < kMaxColors) used |= 1u << cj;
+          } else if ((((unsigned long long)(ia[j + 1] - ia[j]) << 32) |
+                      color_hash((unsigned)j)) > pi) {
+            blocked = true;
+          }
+        }
+      }
+      if (__syncthreads_or(blocked)) {
+        blocked = true;
+        break;
+      }
+    }
+    if (used) atomicOr(&s_used, used);
+    __syncthreads();
+    if (threadIdx.x == 0 && !blocked) {
+      const unsigned u = s_used;
+      const int c = (u == 0xffffffffu) ? kMaxColors : __ffs(~u) - 1;
+      newc[i] = c < cap ? c : kMaxColors;
+      atomicAdd(counter, 1);
+    }
+    __syncthreads();
   }
 }
 
@@ -282,10 +331,14 @@ void Solver::color_level(Level& L, int smoother) {
     ctr.zero();
     BN_LAUNCH(k_color_round, g, 256, 0, s, L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, n,
               color.p, newc.p, ctr.p, cap, kColorLong);
-    if (nlong_rows > 0)
+    if (nlong_rows > 0) {
       BN_LAUNCH(k_color_round_long, grid_for((long long)nlong_rows * 32, 256), 256, 0, s,
                 L.A.ia.p, L.A.ja.p, cf_split ? set.p : nullptr, lrows.p, nlong_rows, color.p,
                 newc.p, ctr.p, cap);
+      BN_LAUNCH(k_color_round_huge, nlong_rows < 1024 ? nlong_rows : 1024, 512, 0, s, L.A.ia.p,
+                L.A.ja.p, cf_split ? set.p : nullptr, lrows.p, nlong_rows, color.p, newc.p,
+                ctr.p, cap);
+    }
     BN_LAUNCH(k_color_commit, g, 256, 0, s, n, newc.p, color.p);
     done += read_scalar(ctr.p, s);
     round++;
@@ -414,18 +467,26 @@ void Solver::build_solve_layout() {
   }
   for (int l = 0; l < nl; l++) {
     Level& L = *lv[l];
-    permute_csr(L.A, L.perm.p, L.inv.p, L.Ap, s);
-    analyze_rows(L.Ap, L.layA, s);
-    // row tiles in original row order: classes interleave, x gathers stay local
-    if (coloured_level(l)) order_tiles(L.Ap.n, L.perm.p, L.layA, s);
+    {
+      Phase p1("layout permute A", s, l);
+      permute_csr(L.A, L.perm.p, L.inv.p, L.Ap, s);
+    }
+    {
+      Phase p2("layout rows+tiles A", s, l);
+      analyze_rows(L.Ap, L.layA, s);
+      // row tiles in original row order: classes interleave, x gathers stay local
+      if (coloured_level(l)) order_tiles(L.Ap.n, L.perm.p, L.layA, s);
+    }
     if (l < nl - 1) {
       Level& C = *lv[l + 1];
+      Phase p3("layout P, R", s, l);
       permute_csr(L.P, L.perm.p, C.inv.p, L.Pp, s);
       permute_csr(L.R, C.perm.p, L.inv.p, L.Rp, s);
       analyze_rows(L.Pp, L.layP, s);
       analyze_rows(L.Rp, L.layR, s);
       if (coloured_level(l)) order_tiles(L.Pp.n, L.perm.p, L.layP, s);
       if (coloured_level(l + 1)) order_tiles(L.Rp.n, C.perm.p, L.layR, s);
+      p3.done();
       if (opt.smoother == SMOOTHER_L1) {
         L.l1.alloc(L.A.n, s);
         BN_LAUNCH(k_l1_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.val.p, L.A.n,
