@@ -13,12 +13,16 @@
 // (atomicCAS) and counts the new keys.  Pass 2 keeps the reference's
 // sequential order without serialising the memory traffic: the 32 lanes walk
 // A row i1 together (coalesced), form r*a, expand their P rows into an
-// ordered product stream in shared memory (warp prefix sum), and lane 0
-// consumes the stream in order -- column -> slot lookup, first product
-// assigned, later ones added -- so every sum is formed in exactly the
-// reference's order.  Rows whose column count exceeds the per-warp table use
-// a one-warp block with a large dynamic table, and beyond that a table in
-// global memory.
+// ordered product stream in shared memory (warp prefix sum), and consume the
+// stream 32 products at a time: lanes holding the same column group up
+// (match_any) and the group's first lane adds the group's products, in
+// stream order, to that column's sum (a new column takes its first product
+// and the next slot in order of first appearance), so every sum is formed in
+// exactly the reference's order while distinct columns proceed in parallel.
+// Rows with at most 64 products use small per-warp tables (many resident
+// warps); rows whose column count exceeds the per-warp table use a one-warp
+// block with a large dynamic table, and beyond that a table in global
+// memory.
 #include "internal.cuh"
 
 #include <cub/cub.cuh>
@@ -52,22 +56,6 @@ __device__ __forceinline__ bool table_insert_atomic(Table t, int key) {
     int prev = atomicCAS(&t.keys[h], -1, key);
     if (prev == -1) return true;
     if (prev == key) return false;
-    h = (h + 1) & t.mask;
-  }
-}
-
-// sequential (single lane) find-or-insert; returns the slot
-__device__ __forceinline__ int table_slot(Table t, int key, int new_slot, bool* inserted) {
-  unsigned h = rap_hash(key, t.mask);
-  while (true) {
-    int k = t.keys[h];
-    if (k == key) { *inserted = false; return t.slots[h]; }
-    if (k == -1) {
-      t.keys[h] = key;
-      t.slots[h] = new_slot;
-      *inserted = true;
-      return new_slot;
-    }
     h = (h + 1) & t.mask;
   }
 }
@@ -141,6 +129,28 @@ __device__ int rap_count_row(int ic, Table t, int lane, const int* __restrict__ 
   return cnt;
 }
 
+// read-only probe: slot of key, or -1
+__device__ __forceinline__ int table_find_slot(Table t, int key) {
+  unsigned h = rap_hash(key, t.mask);
+  while (true) {
+    const int k = t.keys[h];
+    if (k == key) return t.slots[h];
+    if (k == -1) return -1;
+    h = (h + 1) & t.mask;
+  }
+}
+// insert a key known to be absent (lanes insert distinct keys concurrently)
+__device__ __forceinline__ void table_put(Table t, int key, int slot) {
+  unsigned h = rap_hash(key, t.mask);
+  while (true) {
+    if (atomicCAS(&t.keys[h], -1, key) == -1) {
+      t.slots[h] = slot;
+      return;
+    }
+    h = (h + 1) & t.mask;
+  }
+}
+
 template <int BUF = kBuf>
 __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
                              const int* __restrict__ ria, const int* __restrict__ rja,
@@ -151,14 +161,13 @@ __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
                              double* __restrict__ cval) {
   table_clear(t, lane);
   __syncwarp();
-  int nslots = 0;
   if (lane == 0) {
-    bool ins;
-    table_slot(t, ic, 0, &ins);
+    table_put(t, ic, 0);
     t.vals[0] = 0.0;
     cja[cbase] = ic;
-    nslots = 1;
   }
+  __syncwarp();
+  int nslots = 1;  // warp-uniform
   const unsigned lt = (1u << lane) - 1u;
   for (int k1 = ria[ic]; k1 < ria[ic + 1]; k1++) {
     const double r = rval[k1];
@@ -192,27 +201,41 @@ __device__ void rap_fill_row(int ic, Table t, int lane, int* bcol, double* bval,
           }
         }
         __syncwarp();
-        if (lane == 0) {
-          const int m = min(BUF, total - cs);
-          for (int q = 0; q < m; q++) {
-            const int col = bcol[q];
-            const double v = bval[q];
-            bool ins;
-            const int slot = table_slot(t, col, nslots, &ins);
-            if (ins) {
-              t.vals[slot] = v;
+        // consume the stream in order, 32 products at a time: lanes holding
+        // the same column form a group whose lowest lane adds the group's
+        // products to that column's sum in stream order (a new column takes
+        // its first product and the next slot, numbered in order of first
+        // appearance); distinct columns proceed in parallel
+        const int m = min(BUF, total - cs);
+        for (int q0 = 0; q0 < m; q0 += 32) {
+          const int q = q0 + lane;
+          const bool act = q < m;
+          const int col = act ? bcol[q] : -1 - lane;
+          const unsigned grp = __match_any_sync(0xffffffffu, col);
+          const bool lead = act && (__ffs(grp) - 1 == lane);
+          int slot = lead ? table_find_slot(t, col) : 0;
+          const unsigned newm = __ballot_sync(0xffffffffu, lead && slot < 0);
+          if (lead) {
+            double acc;
+            unsigned g = grp;
+            if (slot < 0) {
+              slot = nslots + __popc(newm & lt);
+              table_put(t, col, slot);
               cja[cbase + slot] = col;
-              nslots++;
+              acc = bval[q];
+              g &= g - 1;
             } else {
-              t.vals[slot] = xadd(t.vals[slot], v);
+              acc = t.vals[slot];
             }
+            for (; g; g &= g - 1) acc = xadd(acc, bval[q0 + __ffs(g) - 1]);
+            t.vals[slot] = acc;
           }
+          nslots += __popc(newm);
+          __syncwarp();
         }
-        __syncwarp();
       }
     }
   }
-  nslots = __shfl_sync(0xffffffffu, nslots, 0);
   for (int q = lane; q < nslots; q += 32) cval[cbase + q] = t.vals[q];
   __syncwarp();
 }
