@@ -112,6 +112,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "amg_solver_solve_device": (i, [vp, vp, vp, d, i, i]),
         "amg_solver_solve_batch": (i, [vp, i, vp, vp, d, i, vp]),
         "amg_solver_solve_segmented": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
+        "amg_solver_solve_block": (i, [vp, i, vp, vp, d, i, vp, vp]),
+        "amg_solver_solve_block_device": (i, [vp, i, vp, vp, d, i, vp, vp]),
         "amg_solver_solve_segmented_device": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
         "amg_solver_precond": (i, [vp, vp, vp]),
         "amg_solver_size": (i, [vp]),
@@ -250,6 +252,20 @@ class AMGSolver:
         if rc not in (0, -4):
             raise AMGError(rc, self.lib.amg_solver_last_error().decode())
         return X, its
+
+    def solve_block(self, B, X0=None, tol=1e-8, maxiter=200):
+        """The columns of the n x k array B (k <= 64) solved together, each
+        with its own PCG; returns (X, iterations, relres, status)."""
+        B = np.asfortranarray(B, dtype=np.float64).reshape(self.n, -1, order="F")
+        k = B.shape[1]
+        X = (np.zeros((self.n, k), order="F") if X0 is None
+             else np.array(X0, dtype=np.float64, order="F", copy=True).reshape(self.n, k, order="F"))
+        its, rel = np.zeros(k, np.int32), np.zeros(k)
+        rc = self.lib.amg_solver_solve_block(self.h, k, _p(B), _p(X), tol, maxiter, _p(its),
+                                             _p(rel))
+        if rc not in (0, -4, -5):
+            raise AMGError(rc, self.lib.amg_solver_last_error().decode())
+        return X, its, rel, rc
 
     def solve_segmented(self, seg_ptr, b, x0=None, tol=1e-8, maxiter=200):
         """Block-diagonal independent systems (segment k: rows seg_ptr[k] ..

@@ -276,6 +276,11 @@ DevMat<T> Solver::mat(const CSR& M, const DBuf<float>* v32, const RowLayout* lay
   return d;
 }
 
+template DevMat<double> Solver::mat<double>(const CSR&, const DBuf<float>*,
+                                            const RowLayout*) const;
+template DevMat<float> Solver::mat<float>(const CSR&, const DBuf<float>*,
+                                          const RowLayout*) const;
+
 template <class T>
 PackedMat<T> Solver::pmat(const CSR& M, const DBuf<float>& v32, const Packing& pk) const {
   PackedMat<T> d;

@@ -51,6 +51,8 @@ struct Level {
   DBuf<float> b32, x32, r32;
 };
 
+struct BlockWork;  // work vectors of a many-right-hand-side solve (block.cu)
+
 struct Solver {
   int device = 0;
   cudaStream_t s = 0;
@@ -102,6 +104,15 @@ struct Solver {
   template <class T> void precond_t(const T* g, T* out);
   void precond(const double* g, double* out);  // z = M g (FP64 interface)
   int pcg(const double* d_b, double* d_x, double tol, int maxiter, int print_level);
+  // K right-hand sides at once (column-major n x K device arrays), each
+  // column with its own PCG; the V-cycle and IC(0) run on all columns
+  int pcg_block(int K, const double* d_B, double* d_X, double tol, int maxiter, int* h_iters,
+                double* h_relres);
+  template <class T> void smooth_block(BlockWork& W, int l, const T* bb, T* xl, bool forward);
+  template <class T> void backslash_block(BlockWork& W, int l, const T* bb, T* xl);
+  template <class T> void fwdslash_block(BlockWork& W, int l, const T* bb, T* xl);
+  template <class T> void precond_block_t(BlockWork& W, const T* g, T* out);
+  void precond_block(BlockWork& W, const double* g, double* out);
   // independent block-diagonal systems (natural row ranges d_ptr[k]..d_ptr[k+1]-1),
   // each with its own PCG scalars and stopping test; device b, x
   int pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double* d_x, double tol,

@@ -230,6 +230,9 @@ CONFIGS = {
     # segments; HMIS, theta 0.5
     "vascular_20m": dict(depth=22, n_nodes=20_000_000, diffusive_fraction=0.3,
                          coarsening="hmis", theta=0.5),
+    # 5M nodes, the many-right-hand-side workload: trees of depth 20 + lattice
+    "vascular_5m": dict(depth=20, n_nodes=5_000_000, diffusive_fraction=0.0,
+                        coarsening="pmis", theta=0.25),
     # 4M nodes with the 20M network's options (profiling case: its fine
     # matrix, ~240 MB, is larger than the 126 MB L2 but small on the device)
     "vascular_4m": dict(depth=20, n_nodes=4_000_000, diffusive_fraction=0.3,

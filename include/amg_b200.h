@@ -153,6 +153,20 @@ int amg_write_labeled_solution(const char* path, int n, const int* node, const d
 int amg_solver_solve_batch(void* handle, int k, const double* B, double* X, double tol,
                            int maxiter, int* iterations);
 
+/* Many right-hand sides solved together (the boundary-pressure scenarios of
+ * one network): the PCG of every column runs at once over block vectors, so
+ * each pass over a matrix (SpMV -> SpMM) and each IC(0) level, colour class
+ * and coarse level serves all k columns; every column keeps its own alpha,
+ * beta, stopping test and iteration count.  B and X are column-major n x k
+ * (1 <= k <= 64), X holding the initial guesses.  iterations[j] / relres[j]
+ * (may be NULL): the column's iteration count (-maxiter if not converged)
+ * and true ||b - A x|| / ||b||.  Returns 0, AMG_ERR_NOT_CONVERGED (-4) or
+ * AMG_ERR_NAN (-5).  _device: B and X are device pointers. */
+int amg_solver_solve_block(void* handle, int k, const double* B, double* X, double tol,
+                           int maxiter, int* iterations, double* relres);
+int amg_solver_solve_block_device(void* handle, int k, const double* d_B, double* d_X,
+                                  double tol, int maxiter, int* iterations, double* relres);
+
 /* Independent networks packed block-diagonally into one matrix (no entry
  * couples two segments; checked, AMG_ERR_ARG otherwise): segment k is the
  * row range seg_ptr[k] .. seg_ptr[k+1]-1 (host array of nseg + 1 offsets

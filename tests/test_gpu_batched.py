@@ -115,3 +115,76 @@ def test_segmented_errors():
         S.solve_segmented([0, ptr[1], ptr[1] - 1, n], rhs)
     x, its, rel, rc = S.solve_segmented(ptr, rhs, tol=1e-12, maxiter=2)
     assert rc == -4 and np.all(its == -2)
+
+
+# ------------------------------------------------------------ block PCG
+def _scenarios(net, k, seed=0):
+    """k boundary-pressure scenarios: inlet ~ U(10, 16) kPa, outlet ~ U(1, 3) kPa."""
+    from blood_network_b200.network import assemble
+    rng = np.random.default_rng(seed)
+    B = np.zeros((net.n, k), order="F")
+    for j in range(k):
+        pb = np.array([rng.uniform(10e3, 16e3), rng.uniform(1e3, 3e3)])
+        sysj = assemble(net.n_total, net.seg_u, net.seg_v, net.conductance, net.boundary, pb)
+        B[:, j] = sysj.rhs
+    return B
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+@pytest.mark.parametrize("stop", [amg.STOP_BNORM, amg.STOP_RELRES])
+def test_block_pcg_columns(precision, stop):
+    net = make_config("vascular_20k")
+    k = 6  # padded to 8 inside
+    B = _scenarios(net, k)
+    S = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=precision, stop=stop)
+    X, its, rel, rc = S.solve_block(B, tol=1e-8, maxiter=100)
+    assert rc == 0 and X.shape == (net.n, k)
+    for j in range(k):
+        got = relres(net.indptr, net.indices, net.data, X[:, j], B[:, j])
+        assert abs(got - rel[j]) <= 1e-3 * got + 1e-14
+        if stop == amg.STOP_RELRES:
+            assert got < 1e-8
+        else:
+            assert got < 1e-7
+        x1, it1 = S.solve(B[:, j].copy(), tol=1e-8, maxiter=100)
+        assert abs(int(its[j]) - it1) <= 1
+        assert np.linalg.norm(X[:, j] - x1) <= 1e-5 * np.linalg.norm(x1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_block_columns_do_not_interact(precision):
+    net = make_config("vascular_20k")
+    B = _scenarios(net, 8, seed=3)
+    S = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=precision)
+    X1, its1, _, _ = S.solve_block(B, tol=1e-8)
+    B2 = B.copy()
+    B2[:, 5] *= 1.7
+    B2[:, 6] = 0.0  # a zero column: converged at the start, x stays 0
+    X2, its2, _, _ = S.solve_block(B2, tol=1e-8)
+    for j in (0, 1, 2, 3, 4, 7):
+        assert its1[j] == its2[j] and X1[:, j].tobytes() == X2[:, j].tobytes()
+    assert its2[6] == 0 and not np.any(X2[:, 6])
+    X3, its3, _, _ = S.solve_block(B, tol=1e-8)  # deterministic
+    assert X3.tobytes() == X1.tobytes() and np.array_equal(its1, its3)
+
+
+@pytest.mark.gpu
+def test_block_pcg_hub_rows_and_errors():
+    from test_gpu_hubs import hub_matrix
+    import scipy.sparse as sp
+    n, ia, ja, val = hub_matrix()
+    rng = np.random.default_rng(2)
+    B = rng.standard_normal((n, 3))
+    S = amg.AMGSolver(n, ia, ja, val, threshold=0.5, coarsening=amg.COARSEN_HMIS, min_size=100,
+                      stop=amg.STOP_RELRES)
+    X, its, rel, rc = S.solve_block(B, tol=1e-8, maxiter=100)
+    A = sp.csr_matrix((val, ja, ia), shape=(n, n))
+    assert rc == 0
+    for j in range(3):
+        assert np.linalg.norm(B[:, j] - A @ X[:, j]) <= 1e-8 * np.linalg.norm(B[:, j])
+    with pytest.raises(amg.AMGError):
+        S.solve_block(np.zeros((n, 65)))
+    X, its, rel, rc = S.solve_block(B, tol=1e-14, maxiter=2)
+    assert rc == -4 and np.all(its == -2)
