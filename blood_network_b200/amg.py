@@ -113,6 +113,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "amg_solver_solve_batch": (i, [vp, i, vp, vp, d, i, vp]),
         "amg_solver_solve_segmented": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
         "amg_solver_solve_block": (i, [vp, i, vp, vp, d, i, vp, vp]),
+        "amg_solver_autotune": (i, [vp, i, vp, i]),
         "amg_solver_solve_block_device": (i, [vp, i, vp, vp, d, i, vp, vp]),
         "amg_solver_solve_segmented_device": (i, [vp, i, vp, vp, vp, d, i, vp, vp]),
         "amg_solver_precond": (i, [vp, vp, vp]),
@@ -252,6 +253,15 @@ class AMGSolver:
         if rc not in (0, -4):
             raise AMGError(rc, self.lib.amg_solver_last_error().decode())
         return X, its
+
+    def autotune(self, what=3):
+        """Pick the fastest solve-phase kernel variant per level operator;
+        returns records (level, operator 0 A / 1 R / 2 P / 3 GS, choice, ms)."""
+        rep = np.zeros(4 * 4 * 64)
+        m = self.lib.amg_solver_autotune(self.h, what, _p(rep), rep.shape[0])
+        if m < 0:
+            raise AMGError(m, self.lib.amg_solver_last_error().decode())
+        return rep[:4 * m].reshape(m, 4)
 
     def solve_block(self, B, X0=None, tol=1e-8, maxiter=200):
         """The columns of the n x k array B (k <= 64) solved together, each

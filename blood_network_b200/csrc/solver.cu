@@ -1614,3 +1614,112 @@ BN_API int amg_solver_level_copy(void* h, int level, int* a_ia, int* a_ja, doubl
 BN_API const char* amg_solver_last_error(void) { return bn::t_msg.c_str(); }
 BN_API int amg_solver_last_status(void) { return bn::t_status; }
 BN_API unsigned long long amg_b200_launch_count(void) { return bn::g_launch_count; }
+
+// ------------------------------------------------------------ autotuner
+// Per level, times the candidate kernels of the solve phase on the level's
+// own operators and keeps the fastest:
+//  * SpMV, restriction and prolongation (A, R, P): the row-tile kernel
+//    (group 0) or 4, 8 or 32 lanes per row (the rows-per-warp / vector-width
+//    choice of the row-group kernels);
+//  * Gauss-Seidel colour classes: 1, 8 or 32 lanes per row.
+// Each candidate computes every row sum over the row's entries (tile
+// kernel: in storage order; row groups: lane strides then a fixed shuffle
+// tree), so the choice changes rounding only.  Timed in the precision the
+// solver runs in; operators on the packed kernels keep them.
+namespace bn {
+namespace {
+template <class T>
+double time_ms(cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, int reps,
+               const std::function<void()>& f) {
+  f();
+  cudaEventRecord(e0, s);
+  for (int r = 0; r < reps; r++) f();
+  cudaEventRecord(e1, s);
+  BN_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  return (double)t / reps;
+}
+}  // namespace
+
+template <class T>
+int Solver::autotune_t(int what, double* report, int nreport) {
+  const int nl = (int)lv.size();
+  const int reps = 5;
+  int written = 0;
+  auto note = [&](int l, int op, int choice, double ms) {
+    if (report && written + 4 <= nreport) {
+      report[written++] = l;
+      report[written++] = op;
+      report[written++] = choice;
+      report[written++] = ms;
+    }
+  };
+  for (int l = 0; l + 1 < nl; l++) {
+    Level& L = *lv[l];
+    Level& C = *lv[l + 1];
+    const int n = L.A.n, nc = C.A.n;
+    DBuf<T> u(n, s), v(n, s), w(n, s), cu(nc, s);
+    BN_CUDA(cudaMemsetAsync(u.p, 0, sizeof(T) * n, s));
+    BN_CUDA(cudaMemsetAsync(v.p, 0, sizeof(T) * n, s));
+    BN_CUDA(cudaMemsetAsync(cu.p, 0, sizeof(T) * nc, s));
+    if (what & 1) {
+      struct Op { const CSR* M; const DBuf<float>* v32; RowLayout* lay; bool packed; const T* x;
+                  T* y; int id; };
+      Op ops[3] = {{&L.Ap, &L.A32, &L.layA, L.use_pkA && use_packed, u.p, v.p, 0},
+                   {&L.Rp, &L.R32, &L.layR, L.use_pkR && use_packed, u.p, cu.p, 1},
+                   {&L.Pp, &L.P32, &L.layP, L.use_pkP && use_packed, cu.p, v.p, 2}};
+      for (Op& op : ops) {
+        if (op.packed || op.M->n == 0) continue;
+        int best = op.lay->group;
+        double best_ms = 1e30;
+        for (int g : {0, 4, 8, 32}) {
+          op.lay->group = g;
+          DevMat<T> M = mat<T>(*op.M, op.v32, op.lay);
+          const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
+            spmv<T>(SPMV_Y, M, op.x, nullptr, op.y, s);
+          });
+          if (ms < best_ms) { best_ms = ms; best = g; }
+        }
+        op.lay->group = best;
+        note(l, op.id, best, best_ms);
+      }
+    }
+    if ((what & 2) && L.cptr.size() > 1 && n > kSmallLevel &&
+        (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS) &&
+        !(use_packed && L.use_pkA)) {
+      int best = L.gs_group;
+      double best_ms = 1e30;
+      for (int g : {1, 8, 32}) {
+        L.gs_group = g;
+        const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
+          smooth<T>(l, v.p, u.p, true);
+        });
+        if (ms < best_ms) { best_ms = ms; best = g; }
+      }
+      L.gs_group = best;
+      note(l, 3, best, best_ms);
+    }
+  }
+  drop_graphs();
+  BN_CUDA(cudaStreamSynchronize(s));
+  return written / 4;
+}
+template int Solver::autotune_t<double>(int, double*, int);
+template int Solver::autotune_t<float>(int, double*, int);
+
+}  // namespace bn
+
+// See include/amg_b200.h for the contract.
+BN_API int amg_solver_autotune(void* h, int what, double* report, int nreport) {
+  if (!h) { bn::set_last_error(bn::BN_ERR_ARG, "NULL handle"); return bn::BN_ERR_ARG; }
+  Solver* S = (Solver*)h;
+  return bn::guarded([&]() {
+    BN_CUDA(cudaSetDevice(S->device));
+    if (S->opt.precision == AMG_PREC_MIXED) {
+      if (!S->f32_ready) S->prepare_f32();
+      return S->autotune_t<float>(what, report, nreport);
+    }
+    return S->autotune_t<double>(what, report, nreport);
+  }, bn::BN_ERR_CUDA);
+}

@@ -9,6 +9,7 @@
 #include "../../include/amg_b200.h"
 
 #include <cstdlib>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -113,6 +114,9 @@ struct Solver {
   template <class T> void fwdslash_block(BlockWork& W, int l, const T* bb, T* xl);
   template <class T> void precond_block_t(BlockWork& W, const T* g, T* out);
   void precond_block(BlockWork& W, const double* g, double* out);
+  // times the candidate solve-phase kernels per level and keeps the fastest
+  // (what: 1 SpMV/transfer row groups, 2 Gauss-Seidel lanes per row)
+  template <class T> int autotune_t(int what, double* report, int nreport);
   // independent block-diagonal systems (natural row ranges d_ptr[k]..d_ptr[k+1]-1),
   // each with its own PCG scalars and stopping test; device b, x
   int pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double* d_x, double tol,

@@ -153,6 +153,16 @@ int amg_write_labeled_solution(const char* path, int n, const int* node, const d
 int amg_solver_solve_batch(void* handle, int k, const double* B, double* X, double tol,
                            int maxiter, int* iterations);
 
+/* Autotuner: for every level, times the candidate solve-phase kernels on
+ * the level's own operators in the solver's current precision and keeps the
+ * fastest -- rows per group / vector width of the SpMV, restriction and
+ * prolongation kernels (row tiles, or 4, 8, 32 lanes per row) when what & 1,
+ * lanes per row of the Gauss-Seidel colour classes (1, 8, 32) when what & 2.
+ * The choice changes only the rounding of row sums.  report (may be NULL)
+ * receives up to nreport/4 records {level, operator (0 A, 1 R, 2 P, 3 GS),
+ * choice, ms}; returns the number of records, or a negative status. */
+int amg_solver_autotune(void* handle, int what, double* report, int nreport);
+
 /* Many right-hand sides solved together (the boundary-pressure scenarios of
  * one network): the PCG of every column runs at once over block vectors, so
  * each pass over a matrix (SpMV -> SpMM) and each IC(0) level, colour class

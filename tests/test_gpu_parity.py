@@ -279,3 +279,21 @@ def test_bench_kernel_timings(net20k):
     for which in range(4):
         for prec in (0, 1):
             assert s.bench_kernel(which, prec, reps=3) > 0.0
+
+
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_autotuner_choices(net20k, precision):
+    """amg_solver_autotune keeps, per level operator, the fastest candidate
+    (SpMV row groups 0/4/8/32, GS lanes 1/8/32); the solve still converges
+    with the same work."""
+    s = _solver(net20k.n, net20k.indptr, net20k.indices, net20k.data, precision=precision)
+    x0, it0 = s.solve(net20k.rhs, tol=1e-8)
+    rep = s.autotune(3)
+    assert rep.shape[0] >= 3
+    for lvl, op, choice, ms in rep:
+        assert 0 <= lvl < s.num_levels - 1 and ms > 0
+        assert (choice in (0, 4, 8, 32)) if op < 3 else (choice in (1, 8, 32))
+    x1, it1 = s.solve(net20k.rhs, tol=1e-8)
+    assert abs(it1 - it0) <= 1
+    assert relres(net20k.indptr, net20k.indices, net20k.data, x1, net20k.rhs) <= 1e-8
+    s.close()
