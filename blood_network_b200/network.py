@@ -267,3 +267,17 @@ def block_diagonal(nets):
     rhs = np.concatenate([nt.rhs for nt in nets])
     return (int(seg_ptr[-1]), indptr.astype(np.int32), indices.astype(np.int32), data, rhs,
             seg_ptr.astype(np.int32))
+
+
+def batch_networks(count: int = 256, lo: int = 5_000, hi: int = 200_000, seed: int = 0):
+    """Independent networks of the multi-network batch: node counts
+    log-uniform in [lo, hi], trees of depth round(log2(0.2 n)) (the depth
+    the named configs use for their sizes), seeds seed+1 .. seed+count."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(np.int64)
+    nets = []
+    for k, m in enumerate(sizes):
+        depth = max(4, int(round(np.log2(0.2 * m))))
+        nets.append(vascular_network(depth=depth, n_nodes=int(m), seed=seed + 1 + k,
+                                     keep_segments=False))
+    return nets
