@@ -202,7 +202,18 @@ def run_profile(args):
     net = make_config(args.config, keep_segments=False)
     s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, threshold=cfg["theta"],
                       coarsening=coarsen, precision=amg.PREC_MIXED, stop=amg.STOP_RELRES)
-    if args.profile == "solve":
+    if args.profile == "block":
+        rng = np.random.default_rng(0)
+        B = np.asfortranarray(net.rhs[:, None] * rng.uniform(0.5, 1.5, (1, 16)))
+        s.solve_block(B, tol=1e-8)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("profiled_block")
+        X, its, rel, rc = s.solve_block(B, tol=1e-8)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        print(f"profiled block solve (16 columns): n={net.n} nnz={net.nnz} "
+              f"iterations={int(its.max())} status={rc}", flush=True)
+    elif args.profile == "solve":
         s.solve(net.rhs, tol=1e-8)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_push("profiled_solve")
@@ -309,10 +320,12 @@ def main():
                     help="batched workloads instead of the headline: 64 boundary scenarios on "
                          "the 5M network (block PCG) and 256 networks of 5k-200k nodes "
                          "(segmented PCG), each against one-at-a-time solves")
-    ap.add_argument("--profile", choices=["solve", "spmv", "gs"], default=None,
+    ap.add_argument("--profile", choices=["solve", "spmv", "gs", "block"], default=None,
                     help="profiling driver: 'solve' runs one warm-up and one NVTX-scoped "
                          "('profiled_solve') mixed solve; 'spmv'/'gs' run the fine-level FP64 "
-                         "residual SpMV / FP32 GS sweep three times after setup")
+                         "residual SpMV / FP32 GS sweep three times after setup; 'block' "
+                         "runs one warm-up and one NVTX-scoped ('profiled_block') 16-column "
+                         "block solve")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -1084,6 +1084,7 @@ int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double*
   enum { BB, RR, RZ, RZ0, PAP, RZNEW, RZON, ALPHA, BETA, NSC };
   DBuf<double> scal((size_t)NSC * nseg, s);
   auto S_ = [&](int w) { return scal.p + (size_t)w * nseg; };
+  cudaEventRecord(ev0, s);
   vpermute<double>(d_b, perm0, n0, b.p, false, s);
   vpermute<double>(d_x, perm0, n0, x.p, false, s);
   spmv<double>(SPMV_RES, A, x.p, b.p, r.p, s);  // r = b - A x
@@ -1120,11 +1121,15 @@ int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double*
   seg_dot(ap.p, ap.p, d_ptr, inv0, nseg, S_(RR), s);
   BN_LAUNCH(k_seg_relres, grid_for(nseg, 256), 256, 0, s, S_(RR), S_(BB), nseg, S_(ALPHA));
   vpermute<double>(x.p, perm0, n0, d_x, true, s);
+  cudaEventRecord(ev1, s);
   std::vector<int> hi(2 * (size_t)nseg);
   std::vector<double> hr(nseg);
   BN_CUDA(cudaMemcpyAsync(hi.data(), ints.p, sizeof(int) * 2 * nseg, cudaMemcpyDeviceToHost, s));
   BN_CUDA(cudaMemcpyAsync(hr.data(), S_(ALPHA), sizeof(double) * nseg, cudaMemcpyDeviceToHost, s));
   BN_CUDA(cudaStreamSynchronize(s));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  stats.solve_seconds = ms * 1e-3;
   int worst = 0, failed = 0, nan = 0;
   for (int k = 0; k < nseg; k++) {
     int it = hi[nseg + k];
