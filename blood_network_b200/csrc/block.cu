@@ -35,6 +35,48 @@ template <> __device__ __forceinline__ double bsub(double a, double b) { return 
 template <> __device__ __forceinline__ float bsub(float a, float b) { return __fsub_rn(a, b); }
 
 enum { BM_Y = 0, BM_RES = 1, BM_ADD = 2 };
+constexpr int kLongWarps = 32;  // warps per block for rows longer than kLongRow
+
+// Row sum of a warp over entries k0..k1-1 in storage order: the lanes load
+// 32 entries at a time (one coalesced read of ja and a), then every entry is
+// broadcast by shuffle and each lane accumulates its columns, so the x
+// gathers of consecutive entries do not wait on one another's index loads.
+// SUB: s -= a_ij x_j (triangular rows) instead of s += ; DIAG >= 0: the
+// entry with column DIAG is not summed, its value goes to *d.
+template <class T, bool SUB>
+__device__ __forceinline__ void warp_row_sum(int k0, int k1, const int* __restrict__ ja,
+                                             const T* __restrict__ a, const T* X, int K,
+                                             int lane, bool c0, bool c1, int diag, T& s0, T& s1,
+                                             T* d, bool* hit = nullptr) {
+  for (int base = k0; base < k1; base += 32) {
+    const int kk = base + lane;
+    int jv = 0;
+    T av = T(0);
+    if (kk < k1) {
+      jv = ja[kk];
+      av = a[kk];
+    }
+    const int m = min(32, k1 - base);
+#pragma unroll 4
+    for (int e = 0; e < m; e++) {
+      const int j = __shfl_sync(0xffffffffu, jv, e);
+      const T v = __shfl_sync(0xffffffffu, av, e);
+      if (j == diag) {  // uniform over the warp (j is broadcast)
+        *d = v;
+        if (hit) *hit = true;
+        continue;
+      }
+      const T* xr = X + (size_t)j * K;
+      if (SUB) {
+        if (c0) s0 = bsub(s0, bmul(v, xr[lane]));
+        if (c1) s1 = bsub(s1, bmul(v, xr[lane + 32]));
+      } else {
+        if (c0) s0 = badd(s0, bmul(v, xr[lane]));
+        if (c1) s1 = badd(s1, bmul(v, xr[lane + 32]));
+      }
+    }
+  }
+}
 
 // ---------------------------------------------------------------- SpMM
 // Y = A X | B - A X | Y + A X for the rows of [0, n) (rows longer than
@@ -50,12 +92,7 @@ k_spmm(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
     const int k0 = ia[i], k1 = ia[i + 1];
     if (skip_long && k1 - k0 > kLongRow) continue;
     T s0 = T(0), s1 = T(0);
-    for (int k = k0; k < k1; k++) {
-      const T v = a[k];
-      const T* xr = X + (size_t)ja[k] * K;
-      if (c0) s0 = badd(s0, bmul(v, xr[lane]));
-      if (c1) s1 = badd(s1, bmul(v, xr[lane + 32]));
-    }
+    warp_row_sum<T, false>(k0, k1, ja, a, X, K, lane, c0, c1, -1, s0, s1, nullptr);
     T* yr = Y + (size_t)i * K;
     const T* br = B ? B + (size_t)i * K : nullptr;
     if (c0) yr[lane] = MODE == BM_Y ? s0 : (MODE == BM_RES ? bsub(br[lane], s0) : badd(yr[lane], s0));
@@ -65,30 +102,35 @@ k_spmm(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
   }
 }
 
-// a block of kBlkWarps warps per long row: warp w sums entries k0+w, k0+w+8, ...
+// a block of kLongWarps warps per long row: warp w sums the w-th of
+// kLongWarps consecutive pieces of the row (storage order within a piece),
+// the pieces' sums are combined in piece order
+__device__ __forceinline__ void long_piece(int k0, int k1, int w, int* p0, int* p1) {
+  const int len = k1 - k0, per = (len + kLongWarps - 1) / kLongWarps;
+  *p0 = min(k1, k0 + w * per);
+  *p1 = min(k1, *p0 + per);
+}
+
 template <class T, int MODE>
-__global__ void __launch_bounds__(32 * kBlkWarps)
+__global__ void __launch_bounds__(32 * kLongWarps)
 k_spmm_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
             const int* __restrict__ lrows, int nl, const T* __restrict__ X,
             const T* __restrict__ B, T* __restrict__ Y, int K) {
-  __shared__ T part[kBlkWarps][kMaxK];
+  __shared__ T part[kLongWarps][kMaxK];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const bool c0 = lane < K, c1 = lane + 32 < K;
   for (int q = blockIdx.x; q < nl; q += gridDim.x) {
     const int i = lrows[q];
     T s0 = T(0), s1 = T(0);
-    for (int k = ia[i] + w; k < ia[i + 1]; k += kBlkWarps) {
-      const T v = a[k];
-      const T* xr = X + (size_t)ja[k] * K;
-      if (c0) s0 = badd(s0, bmul(v, xr[lane]));
-      if (c1) s1 = badd(s1, bmul(v, xr[lane + 32]));
-    }
+    int p0, p1;
+    long_piece(ia[i], ia[i + 1], w, &p0, &p1);
+    warp_row_sum<T, false>(p0, p1, ja, a, X, K, lane, c0, c1, -1, s0, s1, nullptr);
     part[w][lane] = s0;
     part[w][lane + 32] = s1;
     __syncthreads();
     if (w == 0) {
       T t0 = T(0), t1 = T(0);
-      for (int u = 0; u < kBlkWarps; u++) {
+      for (int u = 0; u < kLongWarps; u++) {
         t0 = badd(t0, part[u][lane]);
         t1 = badd(t1, part[u][lane + 32]);
       }
@@ -113,21 +155,21 @@ void spmm(int mode, const DevMat<T>& A, const T* X, const T* B, T* Y, int K, cud
     case BM_Y:
       BN_LAUNCH((k_spmm<T, BM_Y>), g, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.n, X, B, Y, K, skip);
       if (skip)
-        BN_LAUNCH((k_spmm_long<T, BM_Y>), gl, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
+        BN_LAUNCH((k_spmm_long<T, BM_Y>), gl, 32 * kLongWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
                   A.nlong, X, B, Y, K);
       break;
     case BM_RES:
       BN_LAUNCH((k_spmm<T, BM_RES>), g, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.n, X, B, Y, K,
                 skip);
       if (skip)
-        BN_LAUNCH((k_spmm_long<T, BM_RES>), gl, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
+        BN_LAUNCH((k_spmm_long<T, BM_RES>), gl, 32 * kLongWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
                   A.nlong, X, B, Y, K);
       break;
     default:
       BN_LAUNCH((k_spmm<T, BM_ADD>), g, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.n, X, B, Y, K,
                 skip);
       if (skip)
-        BN_LAUNCH((k_spmm_long<T, BM_ADD>), gl, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
+        BN_LAUNCH((k_spmm_long<T, BM_ADD>), gl, 32 * kLongWarps, 0, s, A.ia, A.ja, A.val, A.lrows,
                   A.nlong, X, B, Y, K);
       break;
   }
@@ -148,14 +190,7 @@ k_gsm(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restric
   for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nshort; t += nw) {
     const int i = r0 + t;
     T s0 = T(0), s1 = T(0), d = T(1);
-    for (int k = ia[i]; k < ia[i + 1]; k++) {
-      const int j = ja[k];
-      const T v = a[k];
-      if (j == i) { d = v; continue; }
-      const T* xr = X + (size_t)j * K;
-      if (c0) s0 = badd(s0, bmul(v, xr[lane]));
-      if (c1) s1 = badd(s1, bmul(v, xr[lane + 32]));
-    }
+    warp_row_sum<T, false>(ia[i], ia[i + 1], ja, a, X, K, lane, c0, c1, i, s0, s1, &d);
     const T* br = B + (size_t)i * K;
     T* o = OUT ? OUT + (size_t)t * K : X + (size_t)i * K;
     if (c0) o[lane] = bsub(br[lane], s0) / d;
@@ -164,11 +199,11 @@ k_gsm(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restric
 }
 
 template <class T>
-__global__ void __launch_bounds__(32 * kBlkWarps)
+__global__ void __launch_bounds__(32 * kLongWarps)
 k_gsm_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
            int r0, int nshort, int nlong, const T* __restrict__ B, T* X, T* __restrict__ OUT,
            int K) {
-  __shared__ T part[kBlkWarps][kMaxK];
+  __shared__ T part[kLongWarps][kMaxK];
   __shared__ T dsh;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const bool c0 = lane < K, c1 = lane + 32 < K;
@@ -176,24 +211,18 @@ k_gsm_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __re
     const int t = nshort + q, i = r0 + t;
     if (threadIdx.x == 0) dsh = T(1);
     __syncthreads();
-    T s0 = T(0), s1 = T(0);
-    for (int k = ia[i] + w; k < ia[i + 1]; k += kBlkWarps) {
-      const int j = ja[k];
-      const T v = a[k];
-      if (j == i) {
-        if (lane == 0) dsh = v;
-        continue;
-      }
-      const T* xr = X + (size_t)j * K;
-      if (c0) s0 = badd(s0, bmul(v, xr[lane]));
-      if (c1) s1 = badd(s1, bmul(v, xr[lane + 32]));
-    }
+    T s0 = T(0), s1 = T(0), d = T(1);
+    int p0, p1;
+    long_piece(ia[i], ia[i + 1], w, &p0, &p1);
+    bool hit = false;
+    warp_row_sum<T, false>(p0, p1, ja, a, X, K, lane, c0, c1, i, s0, s1, &d, &hit);
+    if (hit && lane == 0) dsh = d;  // the warp whose piece holds the diagonal entry
     part[w][lane] = s0;
     part[w][lane + 32] = s1;
     __syncthreads();
     if (w == 0) {
       T t0 = T(0), t1 = T(0);
-      for (int u = 0; u < kBlkWarps; u++) {
+      for (int u = 0; u < kLongWarps; u++) {
         t0 = badd(t0, part[u][lane]);
         t1 = badd(t1, part[u][lane + 32]);
       }
@@ -215,7 +244,7 @@ void gs_class_block(const DevMat<T>& A, int r0, int nr, int nlong, const T* B, T
     BN_LAUNCH(k_gsm<T>, grid_for((long long)nshort * 32, 32 * kBlkWarps, 8), 32 * kBlkWarps, 0, s,
               A.ia, A.ja, A.val, r0, nshort, B, X, OUT, K);
   if (nlong > 0)
-    BN_LAUNCH(k_gsm_long<T>, nlong < 4096 ? nlong : 4096, 32 * kBlkWarps, 0, s, A.ia, A.ja, A.val,
+    BN_LAUNCH(k_gsm_long<T>, nlong < 4096 ? nlong : 4096, 32 * kLongWarps, 0, s, A.ia, A.ja, A.val,
               r0, nshort, nlong, B, X, OUT, K);
 }
 
@@ -276,12 +305,7 @@ __device__ __forceinline__ void tri_row_m(int t, const int* __restrict__ ia,
   const bool c0 = lane < K, c1 = lane + 32 < K;
   T s0 = c0 ? in[(size_t)i * K + lane] : T(0);
   T s1 = c1 ? in[(size_t)i * K + lane + 32] : T(0);
-  for (int k = ia[t]; k < ia[t + 1]; k++) {
-    const T v = val[k];
-    const T* xr = x + (size_t)ja[k] * K;
-    if (c0) s0 = bsub(s0, bmul(v, xr[lane]));
-    if (c1) s1 = bsub(s1, bmul(v, xr[lane + 32]));
-  }
+  warp_row_sum<T, true>(ia[t], ia[t + 1], ja, val, x, K, lane, c0, c1, -1, s0, s1, nullptr);
   const T d = diag[t];
   if (c0) x[(size_t)i * K + lane] = s0 / d;
   if (c1) x[(size_t)i * K + lane + 32] = s1 / d;
