@@ -816,13 +816,25 @@ static void hub_finish(const int* rows, HubStream& H, CSR& Ac, cudaStream_t s) {
 // 1 (<= kBigCap/2), 2 (beyond)
 __global__ void k_rap_classify(const long long* __restrict__ est, int nc, int cap_limit,
                                int* __restrict__ lists, int* __restrict__ counts) {
-  for (int ic = blockIdx.x * blockDim.x + threadIdx.x; ic < nc; ic += gridDim.x * blockDim.x) {
-    long long e = est[ic];
-    if (e < 0) continue;  // handled elsewhere
-    if (e > cap_limit) e = cap_limit;
-    int c = e <= kSmallCap / 2 ? 3 : (e <= kWarpCap / 2 ? 0 : (e <= kBigCap / 2 ? 1 : 2));
-    int pos = atomicAdd(&counts[c], 1);
-    lists[(size_t)c * nc + pos] = ic;
+  // warp-aggregated appends: one atomic per class present in the warp
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < nc; base += stride) {
+    const int ic = base + threadIdx.x;
+    int c = -1;
+    if (ic < nc) {
+      long long e = est[ic];
+      if (e >= 0) {  // e < 0: handled elsewhere
+        if (e > cap_limit) e = cap_limit;
+        c = e <= kSmallCap / 2 ? 3 : (e <= kWarpCap / 2 ? 0 : (e <= kBigCap / 2 ? 1 : 2));
+      }
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, c);
+    const int leader = __ffs(grp) - 1;
+    int pos0 = 0;
+    if (lane == leader && c >= 0) pos0 = atomicAdd(&counts[c], __popc(grp));
+    pos0 = __shfl_sync(0xffffffffu, pos0, leader);
+    if (c >= 0) lists[(size_t)c * nc + pos0 + __popc(grp & ((1u << lane) - 1u))] = ic;
   }
 }
 

@@ -171,8 +171,18 @@ k_spmv_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __r
 
 __global__ void k_long_rows(const int* __restrict__ ia, int n, int* __restrict__ lrows,
                             int* counter) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if (ia[i + 1] - ia[i] > kLongRow) lrows[atomicAdd(counter, 1)] = i;
+  // warp-aggregated appends (the list is sorted afterwards)
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    const bool lng = i < n && ia[i + 1] - ia[i] > kLongRow;
+    const unsigned m = __ballot_sync(0xffffffffu, lng);
+    if (!m) continue;
+    int pos0 = 0;
+    if (lane == 0) pos0 = atomicAdd(counter, __popc(m));
+    pos0 = __shfl_sync(0xffffffffu, pos0, 0);
+    if (lng) lrows[pos0 + __popc(m & ((1u << lane) - 1u))] = i;
+  }
 }
 
 void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {

@@ -224,13 +224,32 @@ __global__ void k_l1_diag(const int* __restrict__ ia, const double* __restrict__
   }
 }
 
+// diagonal value of each row (the last diagonal entry; 1 if none).  Rows
+// longer than kLongRow are left to k_diag_long (a warp per listed row).
 __global__ void k_diag(const int* __restrict__ ia, const int* __restrict__ ja,
                        const double* __restrict__ a, int n, double* __restrict__ d) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (ia[i + 1] - ia[i] > kLongRow) continue;
     double v = 1.0;
     for (int k = ia[i]; k < ia[i + 1]; k++)
       if (ja[k] == i) v = a[k];
     d[i] = v;
+  }
+}
+__global__ void k_diag_long(const int* __restrict__ ia, const int* __restrict__ ja,
+                            const double* __restrict__ a, const int* __restrict__ rows, int m,
+                            double* __restrict__ d) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < m; q += nw) {
+    const int i = rows[q];
+    int last = -1;
+    for (int base = ia[i]; base < ia[i + 1]; base += 32) {
+      const int k = base + lane;
+      const unsigned hit = __ballot_sync(0xffffffffu, k < ia[i + 1] && ja[k] == i);
+      if (hit) last = base + 31 - __clz(hit);
+    }
+    if (lane == 0) d[i] = last >= 0 ? a[last] : 1.0;
   }
 }
 
@@ -522,6 +541,9 @@ void Solver::build_solve_layout() {
         L.dg.alloc(L.A.n, s);
         BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.ja.p, L.Ap.val.p,
                   L.A.n, L.dg.p);
+        if (L.layA.nlong > 0)
+          BN_LAUNCH(k_diag_long, grid_for((long long)L.layA.nlong * 32, 256), 256, 0, s,
+                    L.Ap.ia.p, L.Ap.ja.p, L.Ap.val.p, L.layA.lrows.p, L.layA.nlong, L.dg.p);
       }
     }
   }
