@@ -112,6 +112,13 @@ struct DBuf {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+// Copies of caller-owned host arrays: large pageable copies go through
+// pinned staging buffers filled or drained by several host threads
+// (host_copy.cu).  copy_h2d returns once the source has been read (the DMA
+// may still run on s); copy_d2h returns with the data in place.
+void copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t s);
+void copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 // Device CSR (0-based, int32 indices).
 struct CSR {
   int n = 0, m = 0;  // rows, cols

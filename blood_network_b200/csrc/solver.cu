@@ -1196,10 +1196,17 @@ void upload_csr(Solver& S, int n, int nnz, const int* ia, const int* ja, const d
   BN_REQUIRE(n > 0 && nnz >= 0 && ia && ja && val, BN_ERR_ARG, "invalid CSR arguments");
   CSR Ain;
   Ain.alloc(n, n, nnz, S.s, true);
-  auto kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  BN_CUDA(cudaMemcpyAsync(Ain.ia.p, ia, sizeof(int) * (n + 1), kind, S.s));
-  BN_CUDA(cudaMemcpyAsync(Ain.ja.p, ja, sizeof(int) * (size_t)nnz, kind, S.s));
-  BN_CUDA(cudaMemcpyAsync(Ain.val.p, val, sizeof(double) * (size_t)nnz, kind, S.s));
+  if (device_ptrs) {
+    BN_CUDA(cudaMemcpyAsync(Ain.ia.p, ia, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, S.s));
+    BN_CUDA(cudaMemcpyAsync(Ain.ja.p, ja, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice,
+                            S.s));
+    BN_CUDA(cudaMemcpyAsync(Ain.val.p, val, sizeof(double) * (size_t)nnz,
+                            cudaMemcpyDeviceToDevice, S.s));
+  } else {
+    copy_h2d(Ain.ia.p, ia, sizeof(int) * (size_t)(n + 1), S.s);
+    copy_h2d(Ain.ja.p, ja, sizeof(int) * (size_t)nnz, S.s);
+    copy_h2d(Ain.val.p, val, sizeof(double) * (size_t)nnz, S.s);
+  }
   int f = validate(Ain.ia.p, Ain.ja.p, n, n, nnz, S.s);
   BN_REQUIRE(!(f & 1), BN_ERR_ARG, "CSR row pointers are not a valid 0-based prefix array");
   BN_REQUIRE(!(f & 2), BN_ERR_ARG, "CSR column index out of range");
@@ -1401,11 +1408,10 @@ BN_API int amg_solver_solve(void* h, const double* b, double* x, double tol, int
     BN_CUDA(cudaSetDevice(S->device));
     const int n = S->n();
     bn::DBuf<double> db(n, S->s), dx(n, S->s);
-    db.upload(b, n);
-    dx.upload(x, n);
+    bn::copy_h2d(db.p, b, sizeof(double) * (size_t)n, S->s);
+    bn::copy_h2d(dx.p, x, sizeof(double) * (size_t)n, S->s);
     out = S->pcg(db.p, dx.p, tol, maxiter, print_level);
-    dx.download(x, n);
-    BN_CUDA(cudaStreamSynchronize(S->s));
+    bn::copy_d2h(x, dx.p, sizeof(double) * (size_t)n, S->s);
     return 0;
   }, -1);
   return rc < 0 ? -maxiter : out;
