@@ -167,3 +167,25 @@ def full_pressure(p, net: DeviceNetwork, interior_of):
     P[mask] = p[io[mask]]
     P[net.bnd.long()] = net.p_bnd
     return P
+
+
+def conductance(logr, length, diffusive):
+    """Segment conductances from log-radius (torch, differentiable): the
+    Poiseuille term pi r^4 / (8 mu L) plus, on diffusive segments (mask 1.0),
+    D pi r^2 / L."""
+    import math
+    import torch
+    from .network import D_DIFFUSION, MU_BLOOD
+    r = torch.exp(logr)
+    g = math.pi * r ** 4 / (8.0 * MU_BLOOD * length)
+    return g + diffusive * (D_DIFFUSION * math.pi * r ** 2 / length)
+
+
+def flow_misfit(logr, dnet: DeviceNetwork, length, diffusive, obs, qhat, interior_of,
+                tol=1e-12):
+    """L = sum over observed segments of (q_e - qhat_e)^2 with q = g (P_u - P_v)."""
+    g = conductance(logr, length, diffusive)
+    p = network_pressure(g, dnet, tol=tol)
+    P = full_pressure(p, dnet, interior_of)
+    q = g * (P[dnet.u.long()] - P[dnet.v.long()])
+    return ((q[obs] - qhat) ** 2).sum()

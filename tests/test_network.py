@@ -38,3 +38,23 @@ def test_named_config_sizes():
     net = make_config("vascular_20k")
     assert 19_000 <= net.n <= 22_000
     assert net.nnz < 8 * net.n
+
+
+def test_batch_networks_sizes_and_determinism():
+    from blood_network_b200.network import batch_networks
+    a = batch_networks(6, lo=2000, hi=20000, seed=4)
+    b = batch_networks(6, lo=2000, hi=20000, seed=4)
+    for x, y in zip(a, b):
+        assert x.n == y.n and x.data.tobytes() == y.data.tobytes()
+    # node counts within the range (interior = total minus the two Dirichlet roots)
+    assert all(1000 <= x.n <= 25000 for x in a)
+
+
+def test_adjoint_conductance_matches_generator():
+    import torch
+    from blood_network_b200.adjoint import conductance
+    from blood_network_b200.network import vascular_network
+    net = vascular_network(depth=6, n_nodes=800, seed=2, diffusive_fraction=0.3)
+    g = conductance(torch.as_tensor(np.log(net.radius)), torch.as_tensor(net.length),
+                    torch.as_tensor(net.diffusive.astype(np.float64))).numpy()
+    assert np.allclose(g, net.conductance, rtol=1e-12, atol=0)
