@@ -314,18 +314,24 @@ def run_adjoint(args, n_nodes=10_000_000, depth=21):
 
 
 def run_batched(args):
-    """Batched workloads (1 GPU): (a) 64 boundary-pressure scenarios of the
-    5M network as one block PCG (per-column scalars, SpMM V-cycle), against
-    the same columns solved one at a time on the same hierarchy; (b) 256
-    networks of 5k-200k nodes packed block-diagonally, one segmented PCG,
-    against each network set up and solved on its own.  Mixed precision,
-    true relative residual 1e-8 per column / network."""
+    """Batched workloads: (a) 64 boundary-pressure scenarios of the 5M network
+    as one block PCG (per-column scalars, SpMM V-cycle), against the same
+    columns solved one at a time on the same hierarchy; (b) 256 networks of
+    5k-200k nodes packed block-diagonally, one segmented PCG, against each
+    network set up and solved on its own.  Mixed precision, true relative
+    residual 1e-8 per column / network.  Under torchrun the columns (a) and
+    the networks (b, bin-packed by nonzeros) are split over the ranks, each
+    rank with its own hierarchy; times are the max over ranks, and the
+    one-at-a-time comparisons run only at N = 1."""
+    rank, ws, local = dist_init(args)
     import torch
-    torch.cuda.set_device(0)
+    torch.cuda.set_device(local)
     from blood_network_b200 import amg
     from blood_network_b200.network import assemble, batch_networks, block_diagonal, make_config
+    from blood_network_b200.shard import partition_columns, partition_networks
     out = {"metric": "batched solves: seconds per right-hand side / per network, mixed AMG-PCG "
-                     "to rtol 1e-8, 1 B200", "impl": "b200", "n_gpus": 1, "data": "synthetic"}
+                     "to rtol 1e-8", "impl": "b200", "n_gpus": ws, "data": "synthetic",
+           "scaling": "strong"}
     # (a) one network, 64 scenarios
     net = make_config("vascular_5m")
     rng = np.random.default_rng(0)
@@ -335,58 +341,77 @@ def run_batched(args):
         pb = np.array([rng.uniform(10e3, 16e3), rng.uniform(1e3, 3e3)])
         B[:, j] = assemble(net.n_total, net.seg_u, net.seg_v, net.conductance, net.boundary,
                            pb).rhs
+    cols = partition_columns(K, ws)[rank]
+    Bm = np.asfortranarray(B[:, cols.start:cols.stop])
     S = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, threshold=0.25,
-                      precision=amg.PREC_MIXED, stop=amg.STOP_RELRES)
+                      precision=amg.PREC_MIXED, stop=amg.STOP_RELRES, device=local)
     S.autotune(3)
     times = []
     for rep in range(args.warmup + args.steps):
-        X, its, rel, rc = S.solve_block(B, tol=1e-8)
+        barrier(ws)
+        X, its, rel, rc = S.solve_block(Bm, tol=1e-8)
         if rep >= args.warmup:
             times.append(S.stats().solve_seconds)
-    blk = statistics.mean(times)
-    single = []
-    for j in range(8):
-        x, it = S.solve(B[:, j].copy(), tol=1e-8)
-        single.append(S.stats().solve_seconds)
-    one = statistics.mean(single)
-    out["rhs_block"] = {"workload": f"vascular_5m n={net.n} nnz={net.nnz}, {K} scenarios "
-                                    "(inlet U(10,16) kPa, outlet U(1,3) kPa)",
-                        "block_s": blk, "s_per_rhs": blk / K, "one_at_a_time_s_per_rhs": one,
-                        "speedup": one / (blk / K), "iterations": [int(its.min()), int(its.max())],
-                        "max_relres": float(rel.max()), "status": int(rc)}
+    blk = max_over_ranks(statistics.mean(times), ws)
+    worst_rel = max_over_ranks(float(rel.max()), ws)
+    worst_rc = max_over_ranks(float(-rc), ws)
+    item = {"workload": f"vascular_5m n={net.n} nnz={net.nnz}, {K} scenarios "
+                        f"(inlet U(10,16) kPa, outlet U(1,3) kPa), {len(cols)} per rank",
+            "block_s": blk, "s_per_rhs": blk / K, "iterations": [int(its.min()), int(its.max())],
+            "max_relres": worst_rel, "status": -int(worst_rc)}
+    if ws == 1:
+        single = []
+        for j in range(8):
+            x, it = S.solve(B[:, j].copy(), tol=1e-8)
+            single.append(S.stats().solve_seconds)
+        one = statistics.mean(single)
+        item.update({"one_at_a_time_s_per_rhs": one, "speedup": one / (blk / K)})
+    out["rhs_block"] = item
     S.close()
-    del net, B
+    del net, B, Bm
     # (b) 256 networks
     nets = batch_networks(256)
-    n, ia, ja, val, rhs, ptr = block_diagonal(nets)
+    parts = partition_networks([nt.nnz for nt in nets], ws)
+    mine = [nets[i] for i in parts[rank]]
+    n, ia, ja, val, rhs, ptr = block_diagonal(mine)
+    barrier(ws)
     S = amg.AMGSolver(n, ia, ja, val, threshold=0.25, precision=amg.PREC_MIXED,
-                      stop=amg.STOP_RELRES)
+                      stop=amg.STOP_RELRES, device=local)
     setup = S.stats().setup_seconds
     times = []
     for rep in range(args.warmup + args.steps):
+        barrier(ws)
         x, its, rel, rc = S.solve_segmented(ptr, rhs, tol=1e-8)
         if rep >= args.warmup:
             times.append(S.stats().solve_seconds)
     seg = statistics.mean(times)
     S.close()
-    sep_setup, sep_solve = 0.0, 0.0
-    for nt in nets:
-        Sk = amg.AMGSolver(nt.n, nt.indptr, nt.indices, nt.data, threshold=0.25,
-                           precision=amg.PREC_MIXED, stop=amg.STOP_RELRES)
-        sep_setup += Sk.stats().setup_seconds
-        Sk.solve(nt.rhs, tol=1e-8)
-        sep_solve += Sk.stats().solve_seconds
-        Sk.close()
-    out["networks_segmented"] = {
-        "workload": f"256 networks, {min(nt.n for nt in nets)}-{max(nt.n for nt in nets)} "
-                    f"interior nodes, {n} rows / {int(ia[-1])} nnz packed",
-        "setup_s": setup, "solve_s": seg, "s_per_network": (setup + seg) / len(nets),
-        "separate_setup_s": sep_setup, "separate_solve_s": sep_solve,
-        "separate_s_per_network": (sep_setup + sep_solve) / len(nets),
-        "speedup": (sep_setup + sep_solve) / (setup + seg),
-        "iterations": [int(its.min()), int(its.max())], "max_relres": float(rel.max()),
-        "status": int(rc)}
-    print(json.dumps(out), flush=True)
+    total = max_over_ranks(setup + seg, ws)
+    item = {"workload": f"256 networks, {min(nt.n for nt in nets)}-{max(nt.n for nt in nets)} "
+                        f"interior nodes, {len(mine)} on rank 0 ({n} rows / {int(ia[-1])} nnz "
+                        "packed)",
+            "setup_s": max_over_ranks(setup, ws), "solve_s": max_over_ranks(seg, ws),
+            "s_per_network": total / len(nets), "iterations": [int(its.min()), int(its.max())],
+            "max_relres": max_over_ranks(float(rel.max()), ws),
+            "status": -int(max_over_ranks(float(-rc), ws))}
+    if ws == 1:
+        sep_setup, sep_solve = 0.0, 0.0
+        for nt in nets:
+            Sk = amg.AMGSolver(nt.n, nt.indptr, nt.indices, nt.data, threshold=0.25,
+                               precision=amg.PREC_MIXED, stop=amg.STOP_RELRES)
+            sep_setup += Sk.stats().setup_seconds
+            Sk.solve(nt.rhs, tol=1e-8)
+            sep_solve += Sk.stats().solve_seconds
+            Sk.close()
+        item.update({"separate_setup_s": sep_setup, "separate_solve_s": sep_solve,
+                     "separate_s_per_network": (sep_setup + sep_solve) / len(nets),
+                     "speedup": (sep_setup + sep_solve) / total})
+    out["networks_segmented"] = item
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 
