@@ -114,7 +114,8 @@ def max_over_ranks(v, ws):
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(v)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(v)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

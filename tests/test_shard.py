@@ -87,3 +87,26 @@ def test_gather_over_two_gloo_ranks():
         mp.spawn(_worker, args=(2, _free_port(), d), nprocs=2, join=True)
         for r in range(2):
             assert open(os.path.join(d, f"rank{r}")).read() == "11"
+
+
+def _bench_worker(rank, ws, port, outdir):
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=ws)
+    try:
+        bench.barrier(ws)
+        m = bench.max_over_ranks(0.5 + rank, ws)  # the bench's max-over-ranks timing
+        with open(os.path.join(outdir, f"rank{rank}"), "w") as f:
+            f.write(repr(m))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_max_over_ranks_on_two_gloo_ranks():
+    import torch.multiprocessing as mp
+    with tempfile.TemporaryDirectory() as d:
+        mp.spawn(_bench_worker, args=(2, _free_port(), d), nprocs=2, join=True)
+        assert [float(open(os.path.join(d, f"rank{r}")).read()) for r in range(2)] == [1.5, 1.5]
