@@ -42,7 +42,7 @@ constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than thi
 constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
 constexpr int kColorHuge = 4096;    // ... and longer than this by a block
-constexpr int kSmallLevel = 2048;  // levels up to this size sweep in one block
+constexpr int kSmallLevel = 2048;  // levels up to this size (without hub rows) sweep in one block
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
                               const int* __restrict__ set, int n, const int* __restrict__ color,
@@ -705,7 +705,9 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
       case SMOOTHER_GS: {
         const int nseg = (int)L.cptr.size() - 1;
         T* tmp = f64 ? (T*)L.r.p : (T*)L.r32.p;
-        if (n <= kSmallLevel) {
+        // small levels sweep in one block, unless they hold hub rows (a warp
+        // per row would serialise a class behind them)
+        if (n <= kSmallLevel && L.layA.nlong == 0) {
           gs_level_block<T>(A, L.d_cptr.p, L.d_cjac.p, nseg, forward, bb, xl, tmp, s);
           break;
         }
