@@ -29,21 +29,27 @@ template <> __device__ __forceinline__ float dsub(float a, float b) { return __f
 // Each thread's tile header (the tile's nonzero range, its own row range,
 // its b_i / y_i and dot weight) is loaded one tile ahead, so those loads are
 // in flight while the current tile computes.
-template <class T, int MODE, bool DOT>
+// ROWS < kRows: tiles of ROWS rows (denser operators, whose kRows-row
+// tiles would overflow the product buffer); a kRows-row tile of the visiting
+// order is taken as kRows/ROWS consecutive smaller tiles, the ones past the
+// last row being empty.
+template <class T, int MODE, bool DOT, int ROWS = kRows>
 __global__ void __launch_bounds__(kRows, 8)
 k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
        const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
        const T* __restrict__ dw, double* __restrict__ partial, int skip_long,
        const int* __restrict__ tiles) {
+  static_assert(ROWS <= kRows && kRows % ROWS == 0, "tile rows must divide kRows");
+  constexpr int SUB = kRows / ROWS;
   __shared__ T prod[kTileNnz];
   __shared__ double red[kRows / 32];
   double dot = 0.0;
-  const int ntiles = (n + kRows - 1) / kRows;
+  const int ntiles = ((n + kRows - 1) / kRows) * SUB;
   int e0 = 0, e1 = 0, k0 = 0, k1 = 0;
   T hb = T(0), hw = T(0);
-  auto head = [&](int t0) {
-    const int t1 = min(t0 + kRows, n);
-    e0 = ia[t0];
+  auto head = [&](int t0) {  // t0 may lie past the last row (an empty tile)
+    const int t1 = min(t0 + ROWS, n);
+    e0 = ia[min(t0, n)];
     e1 = ia[t1];
     const int i = t0 + threadIdx.x;
     if (i < t1) {
@@ -54,12 +60,14 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
       if (DOT) hw = dw[i];
     }
   };
-  auto tile_row = [&](int slot) { return (tiles ? tiles[slot] : slot) * kRows; };
+  auto tile_row = [&](int slot) {
+    return (tiles ? tiles[slot / SUB] : slot / SUB) * kRows + (slot % SUB) * ROWS;
+  };
   int nxt = (int)blockIdx.x < ntiles ? tile_row(blockIdx.x) : 0;
   if ((int)blockIdx.x < ntiles) head(nxt);
   for (int slot = blockIdx.x; slot < ntiles; slot += gridDim.x) {
     const int r0 = nxt;
-    const int r1 = min(r0 + kRows, n);
+    const int r1 = min(r0 + ROWS, n);
     const int i = r0 + threadIdx.x;
     const int ce0 = e0, ce1 = e1, ck0 = k0, ck1 = k1;
     const T cb = hb, cw = hw;
@@ -68,25 +76,26 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
       head(nxt);
     }
     T hold = (MODE == SPMV_Y) ? T(0) : cb;
+    // this thread's row, unless the long-row kernel owns it
+    const bool mine = i < r1 && !(skip_long && ck1 - ck0 > kLongRow);
     if (ce1 - ce0 <= kTileNnz) {
       // matrix entries are read once: evict-first, so that L2 keeps x
 #pragma unroll 4
       for (int k = ce0 + threadIdx.x; k < ce1; k += kRows)
         prod[k - ce0] = dmul(__ldcs(a + k), x[__ldcs(ja + k)]);
       __syncthreads();
-      if (i < r1) {
+      if (mine) {
         for (int k = ck0 - ce0; k < ck1 - ce0; k++)
           hold = (MODE == SPMV_RES) ? dsub(hold, prod[k]) : dadd(hold, prod[k]);
       }
       __syncthreads();
-    } else if (i < r1) {
-      if (skip_long && ck1 - ck0 > kLongRow) continue;  // long-row kernel
+    } else if (mine) {
       for (int k = ck0; k < ck1; k++) {
         T p = dmul(a[k], x[ja[k]]);
         hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
       }
     }
-    if (i < r1) {
+    if (mine) {
       y[i] = hold;
       if (DOT) dot += (double)cw * (double)hold;
     }
@@ -188,6 +197,13 @@ __global__ void k_long_rows(const int* __restrict__ ia, int n, int* __restrict__
 void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {
   const double avg = A.n > 0 ? (double)A.nnz / A.n : 0.0;
   out.group = avg <= 8.0 ? 0 : (avg <= 16.0 ? 4 : (avg <= 48.0 ? 8 : 32));
+  // BN_SPMV_GROUP=g pins every operator to one kernel variant (0-3: row
+  // tiles of 256/128/64/32 rows, 4/8/32: lanes per row); the autotuner may
+  // still change it
+  static const int forced = getenv("BN_SPMV_GROUP") ? atoi(getenv("BN_SPMV_GROUP")) : -1;
+  if (forced == 0 || forced == 1 || forced == 2 || forced == 3 || forced == 4 || forced == 8 ||
+      forced == 32)
+    out.group = forced;
   DBuf<int> cnt(1, s);
   cnt.zero();
   out.lrows.alloc(A.n > 0 ? A.n : 1, s);
@@ -240,6 +256,18 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
     case 0:
       BN_LAUNCH((k_spmv<T, MODE, DOT>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dw,
                 partial, skip, A.tiles);
+      break;
+    case 1:
+      BN_LAUNCH((k_spmv<T, MODE, DOT, 128>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip, A.tiles);
+      break;
+    case 2:
+      BN_LAUNCH((k_spmv<T, MODE, DOT, 64>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip, A.tiles);
+      break;
+    case 3:
+      BN_LAUNCH((k_spmv<T, MODE, DOT, 32>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+                dw, partial, skip, A.tiles);
       break;
     case 4:
       BN_LAUNCH((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,

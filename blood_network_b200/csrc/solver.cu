@@ -1653,9 +1653,9 @@ BN_API unsigned long long amg_b200_launch_count(void) { return bn::g_launch_coun
 // ------------------------------------------------------------ autotuner
 // Per level, times the candidate kernels of the solve phase on the level's
 // own operators and keeps the fastest:
-//  * SpMV, restriction and prolongation (A, R, P): the row-tile kernel
-//    (group 0) or 4, 8 or 32 lanes per row (the rows-per-warp / vector-width
-//    choice of the row-group kernels);
+//  * SpMV, restriction and prolongation (A, R, P): the row-tile kernel with
+//    256, 128, 64 or 32 rows per tile (groups 0-3) or 4, 8 or 32 lanes per
+//    row (the rows-per-warp / vector-width choice of the row-group kernels);
 //  * Gauss-Seidel colour classes: 1, 8 or 32 lanes per row.
 // Each candidate computes every row sum over the row's entries (tile
 // kernel: in storage order; row groups: lane strides then a fixed shuffle
@@ -1708,7 +1708,7 @@ int Solver::autotune_t(int what, double* report, int nreport) {
         if (op.packed || op.M->n == 0) continue;
         int best = op.lay->group;
         double best_ms = 1e30;
-        for (int g : {0, 4, 8, 32}) {
+        for (int g : {0, 1, 2, 3, 4, 8, 32}) {
           op.lay->group = g;
           DevMat<T> M = mat<T>(*op.M, op.v32, op.lay);
           const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {

@@ -156,7 +156,8 @@ int amg_solver_solve_batch(void* handle, int k, const double* B, double* X, doub
 /* Autotuner: for every level, times the candidate solve-phase kernels on
  * the level's own operators in the solver's current precision and keeps the
  * fastest -- rows per group / vector width of the SpMV, restriction and
- * prolongation kernels (row tiles, or 4, 8, 32 lanes per row) when what & 1,
+ * prolongation kernels (row tiles of 256/128/64/32 rows, or 4, 8, 32 lanes
+ * per row) when what & 1,
  * lanes per row of the Gauss-Seidel colour classes (1, 8, 32) when what & 2.
  * The choice changes only the rounding of row sums.  report (may be NULL)
  * receives up to nreport/4 records {level, operator (0 A, 1 R, 2 P, 3 GS),

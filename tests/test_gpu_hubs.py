@@ -240,3 +240,64 @@ def test_symmetrize_huge_rows():
     for a, b in zip(got, want):
         assert np.asarray(a).tobytes() == np.asarray(b, dtype=np.asarray(a).dtype).tobytes()
     s.close()
+
+
+@pytest.mark.gpu
+def test_spmv_dropins_with_a_long_row_among_short_rows():
+    """A row over 1024 entries inside a tile of short rows is summed once
+    (by the long-row kernel), in every SpMV form."""
+    rng = np.random.default_rng(11)
+    n = 3000
+    rows, cols = [], []
+    for i in range(n):
+        c = rng.choice(n, 1100 if i == 100 else 3, replace=False)
+        rows += [i] * len(c)
+        cols += list(c)
+    import scipy.sparse as sp
+    A = sp.csr_matrix((rng.standard_normal(len(rows)), (rows, cols)), shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    ia, ja, val = (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data)
+    lib = amg.load_library()
+    x = rng.standard_normal(n)
+    y0 = rng.standard_normal(n)
+    ax = A @ x
+    y = np.zeros(n)
+    lib.abyvg(amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(y))
+    assert np.allclose(y, ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+    r = np.zeros(n)
+    lib.abyvam(amg._p(y0), amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(r))
+    assert np.allclose(r, y0 - ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+    y2 = y0.copy()
+    lib.abyvcs(amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(y2))
+    assert np.allclose(y2, y0 + ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
+def test_solve_with_a_long_row_in_a_short_tile(precision):
+    """A ring with one node joined to 1,029 others: its row (1,032 entries)
+    shares a 256-row tile of the SpMV with short rows (under the tile's 2,048
+    entries), and the long-row kernel owns it."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(12)
+    n = 20000
+    u = np.arange(n)
+    v = (u + 1) % n
+    hub = 100
+    nb = rng.choice(np.setdiff1d(np.arange(n), [hub - 1, hub, hub + 1]), 1029, replace=False)
+    uu, vv = np.r_[u, np.full(nb.shape, hub)], np.r_[v, nb]
+    w = rng.uniform(0.5, 1.5, uu.shape[0])
+    W = sp.coo_matrix((np.r_[w, w], (np.r_[uu, vv], np.r_[vv, uu])), shape=(n, n)).tocsr()
+    A = (sp.diags(np.asarray(W.sum(1)).ravel() + 1e-2) - W).tocsr()
+    A.sort_indices()
+    ia, ja, val = A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data
+    assert ia[hub + 1] - ia[hub] == 1032  # diagonal, two ring neighbours, 1,029 others
+    t0 = (hub // 256) * 256
+    assert ia[min(t0 + 256, n)] - ia[t0] <= 2048
+    b = rng.standard_normal(n)
+    s = amg.AMGSolver(n, ia, ja, val, precision=precision, stop=amg.STOP_RELRES, min_size=100)
+    x, it = s.solve(b, tol=1e-8, maxiter=100)
+    assert 0 < it <= 40
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    s.close()
