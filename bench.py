@@ -163,10 +163,91 @@ def _sample_job(steps, warmup):
     return net.n, net.nnz, times, tol_used, rr
 
 
+def _ref_networks_job(idx):
+    """Reference C solver (one core) on networks idx of the 256-network
+    batch: summed setup and solve seconds."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import ref as R
+    from blood_network_b200.network import batch_networks
+    nets = batch_networks(256)
+    ts_sum = tv_sum = 0.0
+    worst = 0.0
+    import scipy.sparse as sp
+    for i in idx:
+        nt = nets[i]
+        it, ts, tv, x = R.ref_timed(nt.n, nt.indptr, nt.indices, nt.data, nt.rhs, 0.25, 500, 1, 1,
+                                    1e-8, 500)
+        A = sp.csr_matrix((nt.data, nt.indices, nt.indptr), shape=(nt.n, nt.n))
+        worst = max(worst, float(np.linalg.norm(nt.rhs - A @ x) / np.linalg.norm(nt.rhs)))
+        ts_sum += ts
+        tv_sum += tv
+    return ts_sum, tv_sum, worst
+
+
+def run_reference_batched(args):
+    """The reference C solver (compiled from its sources, one thread per
+    process) on the batched workloads: (a) a bounded sample of the 64
+    scenarios of the 5M network (one hierarchy, 4 columns solved, the per
+    column time scaled to 64); (b) the 256 networks set up and solved one by
+    one on one core, and split over 8 concurrent processes."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import ref as R
+    import scipy.sparse as sp
+    from blood_network_b200.network import assemble, make_config
+    out = {"impl": "reference", "metric": "batched solves: seconds per right-hand side / per "
+           "network, reference C AMG-PCG on the host", "data": "synthetic"}
+    net = make_config("vascular_5m")
+    rng = np.random.default_rng(0)
+    cols = []
+    for j in range(4):  # the first 4 of the B200 arm's 64 scenarios
+        pb = np.array([rng.uniform(10e3, 16e3), rng.uniform(1e3, 3e3)])
+        cols.append(assemble(net.n_total, net.seg_u, net.seg_v, net.conductance, net.boundary,
+                             pb).rhs)
+    t0 = time.perf_counter()
+    S = R.RefSolver(net.n, net.indptr, net.indices, net.data, theta=0.25, min_size=500, nu=1,
+                    coarsening=1)
+    setup = time.perf_counter() - t0
+    A = sp.csr_matrix((net.data, net.indices, net.indptr), shape=(net.n, net.n))
+    times, its, worst = [], [], 0.0
+    for b in cols:
+        t0 = time.perf_counter()
+        x, it = S.solve(b, tol=1e-8)
+        times.append(time.perf_counter() - t0)
+        its.append(int(it))
+        worst = max(worst, float(np.linalg.norm(b - A @ x) / np.linalg.norm(b)))
+    per = statistics.mean(times)
+    out["rhs_block"] = {"workload": f"vascular_5m n={net.n} nnz={net.nnz}, 4 of 64 scenarios",
+                        "setup_s": setup, "s_per_rhs": per, "s_for_64": setup + 64 * per,
+                        "iterations": its, "max_relres": worst, "cores": 1,
+                        "stop": "B-norm 1e-8 (the reference's rule)"}
+    del S, net
+    t0 = time.perf_counter()
+    ts, tv, worst = _ref_networks_job(list(range(256)))
+    seq = time.perf_counter() - t0
+    import multiprocessing as mp
+    shares = [list(range(k, 256, 8)) for k in range(8)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(8) as pool:
+        res = pool.map(_ref_networks_job, shares)
+    par = time.perf_counter() - t0
+    out["networks_segmented"] = {"workload": "256 networks, 5k-200k nodes, each set up and "
+                                             "solved on its own",
+                                 "setup_s": ts, "solve_s": tv, "wall_1_core_s": seq,
+                                 "s_per_network_1_core": seq / 256,
+                                 "wall_8_processes_s": par, "max_relres": worst,
+                                 "host_cores": os.cpu_count()}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.batched:
+        return run_reference_batched(args)
     from blood_network_b200.network import CONFIGS
     nnz_target = 103_215_590  # nnz of the 20M-node workload (seed 0)
     net, times, tol_used, rr = reference_sample(args.steps, args.warmup)
