@@ -64,3 +64,18 @@ def test_create_without_device_fails_loudly():
     assert not h
     assert lib.amg_solver_last_status() == -8   # AMG_ERR_NO_DEVICE
     assert b"device" in lib.amg_solver_last_error()
+
+
+def test_reference_style_c_caller_builds_and_links(tmp_path):
+    """A C program written against the reference wrapper's API compiles
+    against include/amg_b200.h and links with the library (no GPU needed to
+    build; tests/c/drop_in_example.c)."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = os.path.join(root, "blood_network_b200", "lib")
+    exe = str(tmp_path / "drop_in_example")
+    subprocess.run(["gcc", "-std=c99", "-O2", "-Wall", "-Werror",
+                    os.path.join(root, "tests", "c", "drop_in_example.c"),
+                    "-I" + os.path.join(root, "include"), "-L" + lib, "-lamg_b200",
+                    "-Wl,-rpath," + lib, "-lm", "-o", exe], check=True, capture_output=True)
+    assert os.path.exists(exe)
