@@ -1,7 +1,8 @@
 /* A C caller written against the reference wrapper's API (amg_solver_create /
  * amg_solver_solve / amg_solver_free, C_amg1/src/amg_wrapper.c), built
  * unchanged against include/amg_b200.h and linked with libamg_b200.so.
- * Solves a 1D Laplacian (Dirichlet at both ends) and checks the residual. */
+ * Solves a diagonally dominant 1D operator (2.5 on the diagonal, -1 beside
+ * it) and checks the residual. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -19,7 +20,7 @@ int main(int argc, char** argv) {
   for (int i = 0; i < n; i++) {
     ia[i] = nnz;
     if (i > 0) { ja[nnz] = i - 1; val[nnz++] = -1.0; }
-    ja[nnz] = i; val[nnz++] = 2.0;
+    ja[nnz] = i; val[nnz++] = 2.5;
     if (i < n - 1) { ja[nnz] = i + 1; val[nnz++] = -1.0; }
     b[i] = 1.0;
   }
@@ -32,7 +33,7 @@ int main(int argc, char** argv) {
   const int it = amg_solver_solve(h, b, x, 1e-10, 500, 0);
   double r2 = 0.0, b2 = 0.0;
   for (int i = 0; i < n; i++) {
-    double ax = 2.0 * x[i] - (i > 0 ? x[i - 1] : 0.0) - (i < n - 1 ? x[i + 1] : 0.0);
+    double ax = 2.5 * x[i] - (i > 0 ? x[i - 1] : 0.0) - (i < n - 1 ? x[i + 1] : 0.0);
     r2 += (b[i] - ax) * (b[i] - ax);
     b2 += b[i] * b[i];
   }

@@ -79,3 +79,18 @@ def test_reference_style_c_caller_builds_and_links(tmp_path):
                     "-I" + os.path.join(root, "include"), "-L" + lib, "-lamg_b200",
                     "-Wl,-rpath," + lib, "-lm", "-o", exe], check=True, capture_output=True)
     assert os.path.exists(exe)
+
+
+@pytest.mark.gpu
+def test_reference_style_c_caller_runs(tmp_path):
+    """The same C program runs on the GPU and reaches its residual."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib = os.path.join(root, "blood_network_b200", "lib")
+    exe = str(tmp_path / "drop_in_example")
+    subprocess.run(["gcc", "-std=c99", "-O2", os.path.join(root, "tests", "c",
+                                                           "drop_in_example.c"),
+                    "-I" + os.path.join(root, "include"), "-L" + lib, "-lamg_b200",
+                    "-Wl,-rpath," + lib, "-lm", "-o", exe], check=True, capture_output=True)
+    out = subprocess.run([exe, "20000"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "relres=" in out.stdout
