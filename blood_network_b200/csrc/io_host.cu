@@ -13,12 +13,16 @@
 #include "common.cuh"
 #include "../../include/amg_b200.h"
 
+#include <algorithm>
+#include <cctype>
 #include <cerrno>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -30,6 +34,11 @@ struct Text {
   bool load(const char* path) {
     FILE* f = fopen(path, "rb");
     if (!f) return false;
+    if (fseek(f, 0, SEEK_END) == 0) {  // size the buffer once when the file is seekable
+      const long sz = ftell(f);
+      if (sz > 0) buf.reserve((size_t)sz + 1);
+      fseek(f, 0, SEEK_SET);
+    }
     char tmp[1 << 16];
     size_t got;
     while ((got = fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + got);
@@ -57,6 +66,85 @@ struct Text {
   }
 };
 
+// The COO entries of a large file are parsed by several threads: the text
+// is cut at whitespace into one piece per thread, each piece's tokens are
+// counted, and then each thread converts its tokens knowing their global
+// position (token 3k and 3k+1 are the indices of entry k, 3k+2 its value).
+// The conversions are strtoll / strtod as in the one-thread reader, so the
+// result is the same; tokens past entry nz-1 are ignored, as there.
+// Returns -1, or the first entry that cannot be read.
+long long parse_entries(const char* p, const char* end, long long nz, int* r, int* c,
+                        double* v) {
+  const size_t len = (size_t)(end - p);
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = len < (1u << 20) ? 1 : (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+  std::vector<const char*> cut(nt + 1);
+  cut[0] = p;
+  cut[nt] = end;
+  for (int t = 1; t < nt; t++) {
+    const char* q = p + len * t / nt;
+    if (q < cut[t - 1]) q = cut[t - 1];
+    while (q < end && !isspace((unsigned char)*q)) q++;
+    cut[t] = q;
+  }
+  std::vector<long long> count(nt + 1, 0), first_bad(nt, -1);
+  auto run = [&](const std::function<void(int)>& f) {
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(f, t);
+    f(0);
+    for (auto& x : th) x.join();
+  };
+  run([&](int t) {  // tokens per piece
+    long long k = 0;
+    bool in = false;
+    for (const char* q = cut[t]; q < cut[t + 1]; q++) {
+      const bool sp = isspace((unsigned char)*q) || *q == '\0';
+      if (!sp && !in) k++;
+      in = !sp;
+    }
+    count[t + 1] = k;
+  });
+  for (int t = 0; t < nt; t++) count[t + 1] += count[t];
+  const long long need = 3 * nz;
+  run([&](int t) {
+    long long g = count[t];
+    const char* q = cut[t];
+    const char* stop = cut[t + 1];
+    while (g < need) {
+      while (q < stop && (isspace((unsigned char)*q) || *q == '\0')) q++;
+      if (q >= stop) break;
+      const char* tok_end = q;
+      while (tok_end < stop && !isspace((unsigned char)*tok_end) && *tok_end != '\0') tok_end++;
+      char* e = nullptr;
+      bool ok;
+      const long long entry = g / 3;
+      if (g % 3 == 2) {
+        v[entry] = strtod(q, &e);
+        ok = e == tok_end;
+      } else {
+        errno = 0;
+        const long long x = strtoll(q, &e, 10);
+        ok = e == tok_end && !errno && x >= INT32_MIN && x <= INT32_MAX;
+        (g % 3 == 0 ? r : c)[entry] = (int)x;
+      }
+      if (!ok) {
+        first_bad[t] = entry;
+        break;
+      }
+      q = tok_end;
+      g++;
+    }
+  });
+  long long bad = -1;
+  for (int t = 0; t < nt; t++)
+    if (first_bad[t] >= 0 && (bad < 0 || first_bad[t] < bad)) bad = first_bad[t];
+  if (count[nt] < need) {
+    const long long short_at = count[nt] / 3;
+    if (bad < 0 || short_at < bad) bad = short_at;
+  }
+  return bad;
+}
+
 int fail(int code, const std::string& msg) {
   bn::set_last_error(code, msg);
   return code;
@@ -81,17 +169,13 @@ BN_API int amg_read_coo(const char* path, int* nrow, int* ncol, int* nnz, int** 
     return fail(BN_ERR_ARG, "amg_read_coo: cannot read the header \"nrows ncols nnz\"");
   std::vector<int> r((size_t)nz), c((size_t)nz);
   std::vector<double> v((size_t)nz);
+  const long long bad = parse_entries(t.p, t.end, nz, r.data(), c.data(), v.data());
+  if (bad >= 0) return fail(BN_ERR_ARG, "amg_read_coo: cannot read entry " + std::to_string(bad));
   long long lo = 0;
   for (long long k = 0; k < nz; k++) {
-    long long a, b;
-    if (!t.next_int(a) || !t.next_int(b) || !t.next_double(v[k]) || a < INT32_MIN ||
-        a > INT32_MAX || b < INT32_MIN || b > INT32_MAX)
-      return fail(BN_ERR_ARG, "amg_read_coo: cannot read entry " + std::to_string(k));
-    r[k] = (int)a;
-    c[k] = (int)b;
-    if (k == 0) lo = a;
-    if (a < lo) lo = a;
-    if (b < lo) lo = b;
+    if (k == 0) lo = r[k];
+    if (r[k] < lo) lo = r[k];
+    if (c[k] < lo) lo = c[k];
   }
   const int shift = (nz > 0 && lo == 1) ? 1 : 0;  // 1-based file
   std::vector<int> ptr((size_t)m + 1, 0);

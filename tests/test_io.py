@@ -154,3 +154,35 @@ def test_case_solved_and_written(tmp_path):
     io.write_labeled_solution(out, interior, x)
     back = np.loadtxt(out)
     assert np.array_equal(back[:, 0], interior) and np.allclose(back[:, 1], x, rtol=1e-15)
+
+
+def test_large_coo_parsed_in_parallel_matches_reference(tmp_path, oracle):
+    """Files over 1 MB are parsed by several threads (pieces cut at
+    whitespace, tokens placed by their global position): same CSR as the
+    reference's reader, with entries split across lines in odd places."""
+    if not oracle.have_reference():
+        pytest.skip("the reference library was not built here")
+    rng = np.random.default_rng(7)
+    m = n = 5000
+    rows, cols, vals = _random_coo(rng, m, n, 120_000, 1)
+    p = str(tmp_path / "big.txt")
+    with open(p, "w") as f:
+        f.write(f"{m} {n} {len(rows)}\n")
+        for k, (r, c, v) in enumerate(zip(rows, cols, vals)):
+            sep = "\n" if k % 7 == 0 else " "  # some entries span two lines
+            f.write(f"{r}{sep}{c} {v:.17g}\n")
+        f.write("1 2 3 trailing tokens past nnz are ignored\n")
+    assert os.path.getsize(p) > 1 << 20
+    got = io.read_coo(p)
+    want = oracle.ref_read_coo(p)
+    assert got[0] == want[0] and got[1] == want[1]
+    for a, b in zip(got[2:], want[2:]):
+        assert a.tobytes() == b.tobytes()
+    # a malformed entry deep in the file is reported by its index
+    bad = str(tmp_path / "bad_big.txt")
+    with open(bad, "w") as f:
+        f.write(f"{m} {n} 100000\n")
+        for k in range(100_000):
+            f.write(f"{rows[k]} {cols[k]} {'oops' if k == 87_654 else format(vals[k], '.17g')}\n")
+    with pytest.raises(amg.AMGError, match="entry 87654"):
+        io.read_coo(bad)
