@@ -668,7 +668,7 @@ def main():
                               f"n={snet.n}, nnz={snet.nnz}, B-norm tol {tol_used:g} (true relres "
                               f"{rr:.1e}); solve time scaled by nnz ratio {scale:.2f}; setup "
                               f"{statistics.mean(t[0] for t in times) * scale:.1f} s scaled")}
-        except Exception as e:  # the checker library is optional at run time
+        except Exception as e:  # the oracle library is optional at run time
             cpu = {"value": None, "unit": "s", "cores": 1, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 

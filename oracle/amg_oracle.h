@@ -1,7 +1,7 @@
 /*
  * amg_oracle.h -- TEST INFRASTRUCTURE ONLY.  CPU restatement of the
  * reference solver's algorithms (liuzhengqi1996/blood_network, C_amg1), used
- * by tests/ and the smoke check as the checker of the CUDA library, never as
+ * by tests/ and the smoke check as the oracle of the CUDA library, never as
  * the thing measured or shipped.  Every function cites the reference
  * file:line it restates.  Parity of this restatement with the reference is
  * pinned by tests/golden/ (fixtures generated from the compiled reference).

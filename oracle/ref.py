@@ -1,4 +1,4 @@
-"""Test infrastructure: ctypes access to the CPU checkers in this directory.
+"""Test infrastructure: ctypes access to the CPU oracles in this directory.
 
 * ``_ref/libamg_refdrv.so`` -- the reference C_amg1 solver compiled from its
   own sources (see Makefile) plus ref_driver.c, which drives it like
