@@ -120,6 +120,16 @@ def max_over_ranks(v, ws):
     return float(t.item())
 
 
+def solution_rel_error(x, ref):
+    """||x - ref|| / ||ref|| of two tensors, or None when it cannot be formed."""
+    try:
+        import torch
+        den = float(torch.linalg.norm(ref))
+        return float(torch.linalg.norm(x - ref)) / den if den > 0 else None
+    except Exception:
+        return None
+
+
 def barrier(ws):
     if ws > 1:
         import torch.distributed as dist
@@ -594,9 +604,12 @@ def main():
     clocks = ClockSampler(local)
     # FP64 form (beside), then the mixed form (headline) with clocks sampled
     fp64_dev, fp64_its, fp64_rel, _ = solve_steps(amg.PREC_FP64, args.steps, args.warmup)
+    x_fp64 = d_x.clone()  # the FP64 solution, reference for the mixed one
     clocks.start()
     mx_dev, mx_its, mx_rel, launches = solve_steps(amg.PREC_MIXED, args.steps, args.warmup)
     clk = clocks.stop()
+    rel_err = solution_rel_error(d_x, x_fp64)
+    del x_fp64
 
     mixed_s = max_over_ranks(statistics.mean(mx_dev), ws)
     fp64_s = max_over_ranks(statistics.mean(fp64_dev), ws)
@@ -690,6 +703,7 @@ def main():
                        "kernels": "autotuned per level (amg_solver_autotune) before each form",
                        "setup_s": setup_s},
             "fp64_solve_s": fp64_s,
+            "rel_error_vs_fp64_solution": rel_err,
             "mixed_speedup_vs_fp64": fp64_s / mixed_s,
             "iterations": {"mixed": mx_its[-1], "fp64": fp64_its[-1]},
             "relres": {"mixed": max(mx_rel), "fp64": max(fp64_rel)},
