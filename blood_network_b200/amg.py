@@ -25,6 +25,7 @@ STOP_BNORM, STOP_RELRES = 0, 1
 
 STATUS = {0: "OK", -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_OOM", -4: "ERR_NOT_CONVERGED",
           -5: "ERR_NAN", -6: "ERR_SPIN", -7: "ERR_COARSE", -8: "ERR_NO_DEVICE", -9: "ERR_DUP"}
+ERR_ARG, ERR_CUDA, ERR_OOM, ERR_NOT_CONVERGED, ERR_NAN, ERR_SPIN, ERR_COARSE = -1, -2, -3, -4, -5, -6, -7
 
 
 class AMGError(RuntimeError):
@@ -144,6 +145,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ichol_solve": (None, [C.POINTER(IcholFactor), vp, vp]),
         "ichol_free": (None, [C.POINTER(IcholFactor)]),
         "ichol_solve_noalloc": (i, [i, vp, vp, vp, vp, vp, vp]),
+        "amg_debug_wait_timeout": (i, [i, d, C.POINTER(C.c_double)]),
         "amg_build_hierarchy": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat)]),
         "amg_rebuild_values": (None, [C.POINTER(AmgData), C.POINTER(DcsrMat)]),
         "amg_free": (None, [C.POINTER(AmgData)]),

@@ -249,8 +249,7 @@ BN_API void ichol_solve(const ichol_factor* L, const double* b, double* x) {
     ic.solve<double>(db.p, dy.p, dx.p, s);
     dx.download(x, n);
     BN_CUDA(cudaStreamSynchronize(s));
-    int e = ic.take_error(s);
-    BN_REQUIRE(e == 0, e, "IC(0) solve: a bounded dependency wait ran out");
+    ic.check_waits(s);
   });
 }
 

@@ -22,14 +22,19 @@
 // RS / HMIS first pass (parallel counterpart of the sequential bucket greedy
 // at rs_classical.c:108-229 and :390-486; the HMIS PMIS phase, :493-592,
 // never runs because the first pass decides every point): rounds select the
-// undecided local maxima of the RS measure lambda_i (+ a hashed tie-break in
-// [0,1)) over G; undecided points that strongly depend on a new C become F;
+// undecided local maxima of the RS measure lambda_i plus a tie-break in [0,1]
+// over G -- for HMIS the reference's own weights lambda_i + rand()/RAND_MAX
+// after srand(12345), for RS a hash of the index; undecided points that
+// strongly depend on a new C become F;
 // every undecided strong dependency of a new F gains lambda += 1.  The C/F
 // split therefore differs from the sequential greedy's bucket order; the
 // second pass is the reference's (ordered rule above).
 #include "internal.cuh"
 
 #include <stdlib.h>
+#include <string.h>
+
+#include <vector>
 
 namespace bn {
 
@@ -352,6 +357,25 @@ static int count_c(const int* cf, int n, cudaStream_t s) {
   return read_scalar(c.p, s);
 }
 
+// rand() values after srand(12345), drawn from a private generator state:
+// glibc's rand() is random() on its default state (the additive feedback
+// generator with a 128-byte table), and srandom_r/random_r on a table of the
+// same size give the same sequence.
+static void hmis_draws(int* out, int n) {
+  alignas(8) char table[128];
+  struct random_data st;
+  memset(&st, 0, sizeof st);
+  memset(table, 0, sizeof table);
+  BN_REQUIRE(initstate_r(12345u, table, sizeof table, &st) == 0, BN_ERR_ARG,
+             "HMIS: random state");
+  BN_REQUIRE(srandom_r(12345u, &st) == 0, BN_ERR_ARG, "HMIS: random state");
+  for (int i = 0; i < n; i++) {
+    int32_t r;
+    random_r(&st, &r);
+    out[i] = (int)r;
+  }
+}
+
 int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
   (void)max_lam;
   const int n = S.n;
@@ -405,7 +429,24 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
     // RS measure: lambda_i = |S^T_i|; the classical RS routine leaves
     // lambda_0 at zero (rs_classical.c:118-123), reproduced here.
     if (method == COARSEN_RS) BN_CUDA(cudaMemsetAsync(lam.p, 0, sizeof(int), s));
-    BN_LAUNCH(k_rs_measure, g, 256, 0, s, lam.p, n, w.p);
+    std::vector<int> h;
+    DBuf<int> rnd;
+    if (method == COARSEN_HMIS) {
+      // ties between equal measures: the reference HMIS's weights
+      // lambda_i + rand()/RAND_MAX after srand(12345) (rs_classical.c:
+      // 542-551), one draw per point in index order.  The sequence comes
+      // from a private copy of the C library's generator (srandom_r /
+      // random_r, the generator behind srand/rand), so the caller's rand()
+      // state is left alone as the reference's first pass leaves it.
+      h.resize(n);
+      hmis_draws(h.data(), n);
+      rnd.alloc(n, s);
+      rnd.upload(h.data(), n);
+      BN_LAUNCH(k_pmis_weights, g, 256, 0, s, lam.p, rnd.p, n, w.p, cf);
+      BN_CUDA(cudaStreamSynchronize(s));  // h must outlive the copy
+    } else {
+      BN_LAUNCH(k_rs_measure, g, 256, 0, s, lam.p, n, w.p);
+    }
     BN_CUDA(cudaMemsetAsync(cf, 0, sizeof(int) * n, s));
     DBuf<int> new_f(n, s);
     long long undecided = n;

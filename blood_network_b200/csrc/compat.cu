@@ -337,8 +337,7 @@ BN_API void amg_ichol_precond(const amg_data* amg, const dcsr_mat* A, const icho
     S.opt.nu = amg->nu > 0 ? amg->nu : 1;
     S.precond(dg.p, dx.p);
     S.opt.nu = keep;
-    int ic = S.ic.take_error(S.s);
-    BN_REQUIRE(ic == 0, ic, "IC(0) solve: a bounded dependency wait ran out");
+    S.ic.check_waits(S.s);
     bn::from_solve(S, 0, dx.p, x, tmp.p);
     bn::set_last_error(0, "");
     return 0;

@@ -60,45 +60,140 @@ __device__ __forceinline__ unsigned long long value_word(double v) {
 }
 
 constexpr int kFlagThreads = 256;
-constexpr int kSpinFast = 64;          // polls before backing off
-constexpr int kSpinLimit = 1 << 22;    // polls before giving up (seconds with back-off)
+constexpr int kSpinFast = 64;            // polls before backing off
+constexpr int kSpinHardCap = 1 << 27;    // polls: a last bound should the clock not advance
+
+// ------------------------------------------------------------ bounded waits
+// Every wait of a sync-free sweep is bounded in time, and the first wait that
+// runs out abandons the whole launch: it raises the abort word of the
+// sweep's wait record, and every other waiting thread polls that word while
+// it backs off, so a sweep that cannot finish ends within about one limit
+// (not one limit per waiting row).  A wait that gives up uses NaN for the
+// missing value, so the kernel always ends and its output is non-finite.
+//
+// Wait record (kWaitWords ints in device memory, zero between sweeps):
+//   [0] abort word: set by the first wait that gives up
+//   [1] tag of that kernel (WaitTag)
+//   [2] the waiting row (vector index)
+//   [3] the dependency it waited for (vector index)
+//   [4] how long it waited, microseconds
+constexpr int kWaitWords = 8;
+enum WaitTag : int { WT_IC_FWD = 1, WT_IC_BWD = 2, WT_GS_ORDERED = 3, WT_SELFTEST = 4 };
+
+struct WaitCtl {
+  int* rec;                      // the wait record
+  unsigned long long limit_ns;   // give-up time of one wait
+  int tag;                       // WaitTag of the launching sweep
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ int ld_relaxed_i32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The first thread to give up writes the record; later ones only read the
+// abort word.
+__device__ __forceinline__ void wait_give_up(const WaitCtl& w, int row, int dep,
+                                             unsigned long long waited_ns) {
+  if (atomicCAS(w.rec, 0, 1) == 0) {
+    w.rec[1] = w.tag;
+    w.rec[2] = row;
+    w.rec[3] = dep;
+    const unsigned long long us = waited_ns / 1000ull;
+    w.rec[4] = us > 0x7fffffffull ? 0x7fffffff : (int)us;
+  }
+}
+
+// Back-off step of poll number it (it >= kSpinFast): sleeps, and every 16th
+// poll checks the abort word and the time waited.  Returns true when the
+// wait must end now (*ran_out: this wait ran out, rather than another one).
+__device__ __forceinline__ bool wait_backoff(const WaitCtl& w, int it,
+                                             unsigned long long& t0, bool* ran_out) {
+  __nanosleep(it < 4096 ? 32 : 256);
+  if ((it & 15) != 0) return false;
+  if (ld_relaxed_i32(w.rec) != 0) {
+    *ran_out = false;
+    return true;
+  }
+  const unsigned long long t = global_ns();
+  if (t0 == 0) {
+    t0 = t;
+    return false;
+  }
+  if (t - t0 > w.limit_ns || it >= kSpinHardCap) {
+    *ran_out = true;
+    return true;
+  }
+  return false;
+}
 
 // Waits until none of the first m words u[q] (loaded from o[j[q]]) is
 // pending, re-polling all pending ones together so that the last arrival
-// costs one round trip.
+// costs one round trip.  row: the waiting row (for the record).
 template <class U>
 __device__ __forceinline__ void wait_group(const U* o, const int (&j)[4], U (&u)[4], int m,
-                                           U pending, U nan, int* err) {
-  for (int it = 0; it < kSpinLimit; it++) {
+                                           U pending, U nan, const WaitCtl& w, int row) {
+  unsigned long long t0 = 0;
+  for (int it = 0;; it++) {
     bool pend = false;
 #pragma unroll
     for (int q = 0; q < 4; q++) pend |= (q < m && u[q] == pending);
     if (!pend) return;
-    if (it >= kSpinFast) __nanosleep(it < 4096 ? 32 : 256);
+    bool ran_out = false;
+    if (it >= kSpinFast && wait_backoff(w, it, t0, &ran_out)) {
+      int dep = -1;
+#pragma unroll
+      for (int q = 3; q >= 0; q--)
+        if (q < m && u[q] == pending) dep = j[q];
+      if (ran_out) wait_give_up(w, row, dep, global_ns() - t0);
+      break;
+    }
 #pragma unroll
     for (int q = 0; q < 4; q++)
       if (q < m && u[q] == pending) u[q] = ld_relaxed(o + j[q]);
   }
-  atomicExch(err, 1);
 #pragma unroll
   for (int q = 0; q < 4; q++)
     if (q < m && u[q] == pending) u[q] = nan;
 }
 
-// Waits until the word at p (last read as u) is no longer pending (bounded;
-// NaN and an error record when the wait runs out).
+// Waits until the word at o[j] (last read as u) is no longer pending
+// (bounded as above; NaN when the wait is abandoned).
 template <class U>
-__device__ __forceinline__ U wait_word(const U* p, U u, U pending, U nan, int* err) {
-  for (int it = 0; it < kSpinLimit && u == pending; it++) {
-    if (it >= kSpinFast) __nanosleep(it < 4096 ? 32 : 256);
-    u = ld_relaxed(p);
-  }
-  if (u == pending) {
-    atomicExch(err, 1);
-    u = nan;
+__device__ __forceinline__ U wait_word(const U* o, int j, U u, U pending, U nan,
+                                       const WaitCtl& w, int row) {
+  unsigned long long t0 = 0;
+  for (int it = 0; u == pending; it++) {
+    bool ran_out = false;
+    if (it >= kSpinFast && wait_backoff(w, it, t0, &ran_out)) {
+      if (ran_out) wait_give_up(w, row, j, global_ns() - t0);
+      return nan;
+    }
+    u = ld_relaxed(o + j);
   }
   return u;
 }
+
+// Host side of a wait record: the device words, the limit, and the report.
+struct WaitRecord {
+  DBuf<int> rec;
+  unsigned long long limit_ns = default_limit_ns();
+  void init(cudaStream_t s) {  // never inside a stream capture
+    if (!rec.p) rec.alloc(kWaitWords, s);
+    rec.zero();
+  }
+  WaitCtl ctl(int tag) const { return WaitCtl{rec.p, limit_ns, tag}; }
+  // 0, or BN_ERR_SPIN with *msg describing the wait that gave up; the
+  // record is cleared (synchronous on s).
+  int take(cudaStream_t s, std::string* msg);
+  static unsigned long long default_limit_ns();
+};
 
 // 32-row chunks of the level-ordered layout, cut at every level boundary
 inline int upload_chunks(const std::vector<int>& ptr, DBuf<int2>& d, cudaStream_t s) {

@@ -66,7 +66,7 @@ __device__ __forceinline__ void gs_row(int t, int t_end, const int* __restrict__
                                        const double* __restrict__ d, const int* __restrict__ pos,
                                        const int* __restrict__ rows, const double* __restrict__ b,
                                        const double* __restrict__ xin,
-                                       unsigned long long* o, int* err) {
+                                       unsigned long long* o, const WaitCtl& wc) {
   using W = WordOf<double>;
   if (t >= t_end) return;
   const int i = rows[t];
@@ -78,7 +78,7 @@ __device__ __forceinline__ void gs_row(int t, int t_end, const int* __restrict__
     double xj;
     if (pos[j] < pi) {  // updated earlier in this sweep
       unsigned long long u = ld_relaxed(o + j);
-      u = wait_word(o + j, u, W::kPending, W::kNaN, err);
+      u = wait_word(o, j, u, W::kPending, W::kNaN, wc, i);
       xj = word_value(u);
     } else {
       xj = xin[j];
@@ -98,14 +98,14 @@ k_gs_flags(const int* __restrict__ ia, const int* __restrict__ ja, const double*
            const double* __restrict__ d, const int* __restrict__ pos,
            const int* __restrict__ rows, const int2* __restrict__ chunks, int nchunks,
            const double* __restrict__ b, const double* __restrict__ xin, double* xout,
-           int* err) {
+           WaitCtl wc) {
   unsigned long long* o = reinterpret_cast<unsigned long long*>(xout);
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   for (int c = warp; c < nchunks; c += nwarps) {
     const int2 ch = chunks[c];
-    gs_row(ch.x + lane, ch.y, ia, ja, a, d, pos, rows, b, xin, o, err);
+    gs_row(ch.x + lane, ch.y, ia, ja, a, d, pos, rows, b, xin, o, wc);
     __syncwarp();
   }
 }
@@ -118,10 +118,11 @@ void ordered_gs(const CSR& A, const int* d_order, const double* b, double* x, in
   const int n = A.n;
   if (n == 0 || nu <= 0) return;
   const int g = grid_for(n, 256);
-  DBuf<int> pos(n, s), bad(1, s), err(1, s);
+  DBuf<int> pos(n, s), bad(1, s);
+  WaitRecord wait;
+  wait.init(s);
   pos.fill_bytes(0xff);
   bad.zero();
-  err.zero();
   BN_LAUNCH(k_gs_pos, g, 256, 0, s, d_order, n, backward ? 1 : 0, pos.p, bad.p);
   BN_REQUIRE(read_scalar(bad.p, s) == 0, BN_ERR_ARG,
              "ordered Gauss-Seidel: the order is not a permutation of 0..n-1");
@@ -172,13 +173,13 @@ void ordered_gs(const CSR& A, const int* d_order, const double* b, double* x, in
     BN_CUDA(cudaLaunchKernelEx(&cfg, k_gs_flags, (const int*)A.ia.p, (const int*)A.ja.p,
                                (const double*)A.val.p, (const double*)d.p, (const int*)pos.p,
                                (const int*)rows.p, (const int2*)chunks.p, nchunks, b,
-                               (const double*)xin, xout, err.p));
+                               (const double*)xin, xout, wait.ctl(WT_GS_ORDERED)));
     std::swap(xin, xout);
   }
   if (xin != x)
     BN_CUDA(cudaMemcpyAsync(x, xin, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-  BN_REQUIRE(read_scalar(err.p, s) == 0, BN_ERR_SPIN,
-             "ordered Gauss-Seidel: a bounded dependency wait ran out");
+  std::string msg;
+  if (wait.take(s, &msg)) throw Error(BN_ERR_SPIN, "ordered Gauss-Seidel: " + msg);
 }
 
 }  // namespace bn

@@ -28,6 +28,7 @@
 
 #include <cstdlib>
 #include <cstring>
+#include <string>
 
 #include <cooperative_groups.h>
 #include <cub/cub.cuh>
@@ -406,7 +407,7 @@ __global__ void __launch_bounds__(kFlagThreads)
 k_tri_flags(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
             const T* __restrict__ diag, const int* __restrict__ rows,
             const int2* __restrict__ chunks, int nchunks, const T* __restrict__ in, T* out,
-            T* clear, int* err) {
+            T* clear, WaitCtl wc) {
   using W = WordOf<T>;
   using U = typename W::U;
   U* o = reinterpret_cast<U*>(out);
@@ -434,7 +435,7 @@ k_tri_flags(const int* __restrict__ ia, const int* __restrict__ ja, const T* __r
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) u[q] = q < m ? ld_relaxed(o + j[q]) : U(0);
-        wait_group(o, j, u, m, W::kPending, W::kNaN, err);
+        wait_group(o, j, u, m, W::kPending, W::kNaN, wc, i);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           if (q < m) {
@@ -448,6 +449,133 @@ k_tri_flags(const int* __restrict__ ia, const int* __restrict__ ja, const T* __r
       st_relaxed(o + i, r);
     }
     __syncwarp();
+  }
+}
+
+// Tiled form.  Tile q is a range of consecutive row indices; a block takes
+// its tiles in order (the backward sweep numbers the tiles from the end) and
+// walks each tile's levels in order, one step per level with a block
+// barrier after it.  A row's dependencies lie in its own tile at earlier
+// levels (values this block published before a barrier: read through L1)
+// or in earlier tiles (polled like the sync-free form).  Progress: every
+// dependency of a tile lies in the same or an earlier tile, so the earliest
+// unfinished tile always has its block working on it, and within a tile the
+// earliest unfinished step has all its dependencies done.  A stale L1 copy
+// can only hold the pending pattern (each value is written once per sweep,
+// and L1 starts clean at a launch), which the poll loop treats as pending.
+template <class T>
+__global__ void __launch_bounds__(1024)
+k_tri_tiles(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+            const T* __restrict__ diag, const int* __restrict__ rows,
+            const unsigned* __restrict__ imask, const int2* __restrict__ tile_steps,
+            const int2* __restrict__ steps, int ntiles, const T* __restrict__ in, T* out,
+            T* clear, WaitCtl wc) {
+  using W = WordOf<T>;
+  using U = typename W::U;
+  U* o = reinterpret_cast<U*>(out);
+  for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
+    const int2 ts = tile_steps[q];
+    for (int st = ts.x; st < ts.y; st++) {
+      const int2 sp = steps[st];
+      for (int t = sp.x + threadIdx.x; t < sp.y; t += blockDim.x) {
+        const int i = rows[t];
+        const int k0 = ia[t], k1 = ia[t + 1];
+        const unsigned im = imask[t];
+        T s = in[i];
+        const T d = diag[t];
+        if (clear) reinterpret_cast<U*>(clear)[i] = W::kPending;
+        for (int k = k0; k < k1; k += 4) {
+          const int m = k1 - k < 4 ? k1 - k : 4;
+          int j[4];
+          T v[4];
+          U u[4];
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            j[e] = e < m ? ja[k + e] : 0;
+            v[e] = e < m ? val[k + e] : T(0);
+          }
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const int bit = k - k0 + e;
+            const bool own = bit < 32 && ((im >> bit) & 1u);
+            u[e] = e < m ? (own ? __ldca(o + j[e]) : ld_relaxed(o + j[e])) : U(0);
+          }
+          wait_group(o, j, u, m, W::kPending, W::kNaN, wc, i);
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            if (e < m) {
+              if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[e], word_value(u[e])));
+              else s = xsubf(s, xmulf(v[e], word_value(u[e])));
+            }
+          }
+        }
+        U r = value_word(s / d);
+        if (r == W::kPending) r = W::kNaN;
+        st_relaxed(o + i, r);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// schedule of the tiled form (IChol::build_tiles)
+__global__ void k_pos_level(const int* __restrict__ ptr, int nlevels, int n, int* __restrict__ lev) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nlevels - 1;  // last level starting at or before t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ptr[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    lev[t] = lo;
+  }
+}
+// tile of position t: forward = row / R, backward = ntiles - 1 - row / R
+__device__ __forceinline__ int tile_of(int row, int R, int ntiles, bool forward) {
+  const int q = row / R;
+  return forward ? q : ntiles - 1 - q;
+}
+__global__ void k_step_heads(const int* __restrict__ rows, const int* __restrict__ lev, int n,
+                             int R, int ntiles, int forward, int* __restrict__ head) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    int h = 1;
+    if (t > 0)
+      h = lev[t] != lev[t - 1] || tile_of(rows[t], R, ntiles, forward) !=
+                                      tile_of(rows[t - 1], R, ntiles, forward);
+    head[t] = h;
+  }
+}
+__global__ void k_step_tiles(const int* __restrict__ starts, int nsteps,
+                             const int* __restrict__ rows, int R, int ntiles, int forward,
+                             int* __restrict__ tile, int* __restrict__ ids) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nsteps; k += gridDim.x * blockDim.x) {
+    tile[k] = tile_of(rows[starts[k]], R, ntiles, forward);
+    ids[k] = k;
+  }
+}
+__global__ void k_step_ranges(const int* __restrict__ sorted_ids, const int* __restrict__ starts,
+                              int nsteps, int n, const int* __restrict__ sorted_tile,
+                              int2* __restrict__ steps, int2* __restrict__ tile_steps) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nsteps; k += gridDim.x * blockDim.x) {
+    const int id = sorted_ids[k];
+    steps[k] = make_int2(starts[id], id + 1 < nsteps ? starts[id + 1] : n);
+    const int q = sorted_tile[k];
+    if (k == 0 || sorted_tile[k - 1] != q) tile_steps[q].x = k;
+    if (k == nsteps - 1 || sorted_tile[k + 1] != q) tile_steps[q].y = k + 1;
+  }
+}
+// bit e of imask[t]: entry e of row t depends on a row of the same tile
+__global__ void k_tile_mask(const int* __restrict__ ia, const int* __restrict__ ja,
+                            const int* __restrict__ rows, int n, int R,
+                            unsigned* __restrict__ imask) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int q = rows[t] / R;
+    unsigned m = 0;
+    const int k0 = ia[t];
+    const int k1 = min(ia[t + 1], k0 + 32);
+    for (int k = k0; k < k1; k++)
+      if (ja[k] / R == q) m |= 1u << (k - k0);
+    imask[t] = m;
   }
 }
 
@@ -733,14 +861,17 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
     bsrc.alloc((size_t)(fnnz > 0 ? fnnz : 1), s);
     BN_LAUNCH(k_bwd_fill, g, 256, 0, s, U.ia.p, U.ja.p, usrc.p, border.p, n, bia.p, bja.p, bsrc.p);
   }
+  if (mode == kSweepTiles) {
+    build_tiles(true, s);
+    build_tiles(false, s);
+  }
   ph_lay.done();
   {
     Phase ph("ichol values", s);
     refresh_values();
     remap(nullptr, s);
   }
-  err.alloc(1, s);  // here, never inside a stream capture
-  err.zero();
+  wait.init(s);  // here, never inside a stream capture
 }
 
 void IChol::remap(const int* inv, cudaStream_t s) {
@@ -832,7 +963,7 @@ static void run_tri_coop(int nseg, const int4* segs, const int* ia, const int* j
 template <class T>
 static void run_tri_flags(int nchunks, const int2* chunks, int blocks_per_sm, const int* ia,
                           const int* ja, const T* val, const T* diag, const int* rows,
-                          const T* in, T* out, T* clear, int* err, cudaStream_t s) {
+                          const T* in, T* out, T* clear, WaitCtl wc, cudaStream_t s) {
   int dev = 0, per_sm = 0, sms = 0;
   BN_CUDA(cudaGetDevice(&dev));
   BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_flags<T>, kFlagThreads, 0));
@@ -852,7 +983,103 @@ static void run_tri_flags(int nchunks, const int2* chunks, int blocks_per_sm, co
   cfg.numAttrs = 1;
   g_launch_count++;
   BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_flags<T>, ia, ja, val, diag, rows, chunks, nchunks, in,
-                             out, clear, err));
+                             out, clear, wc));
+}
+
+template <class T>
+static void run_tri_tiles(const IChol::Tiles& tl, const int* ia, const int* ja, const T* val,
+                          const T* diag, const int* rows, const T* in, T* out, T* clear,
+                          WaitCtl wc, cudaStream_t s) {
+  int dev = 0, per_sm = 0, sms = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_tiles<T>, tl.threads, 0));
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int cap = sms * per_sm;
+  const int grid = tl.ntiles < cap ? tl.ntiles : cap;
+  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): tiled sweep grid does not fit");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(tl.threads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_tiles<T>, ia, ja, val, diag, rows,
+                             (const unsigned*)tl.imask.p, (const int2*)tl.tile_steps.p,
+                             (const int2*)tl.steps.p, tl.ntiles, in, out, clear, wc));
+}
+
+// The tiled schedule of one sweep direction: tiles of consecutive row
+// indices (as many as the device holds blocks of tl.threads), each tile's
+// rows of one level as one step.
+void IChol::build_tiles(bool forward, cudaStream_t s) {
+  Tiles& tl = forward ? tf : tb;
+  const int* rows = forward ? order.p : border.p;  // natural row ids, layout order
+  const DBuf<int>& dptr = forward ? d_lptr : d_bptr;
+  const int* tia = forward ? fia.p : bia.p;
+  const int* tja = forward ? fja.p : bja.p;
+  static const int threads = getenv("BN_IC_TILE_THREADS") ? atoi(getenv("BN_IC_TILE_THREADS"))
+                                                          : 512;
+  static const int tiles_per_sm =
+      getenv("BN_IC_TILES_PER_SM") ? atoi(getenv("BN_IC_TILES_PER_SM")) : 2;
+  BN_REQUIRE(threads >= 32 && threads <= 1024 && threads % 32 == 0 && tiles_per_sm >= 1,
+             BN_ERR_ARG, "IC(0): tiled sweep shape");
+  int dev = 0, sms = 0, o64 = 0, o32 = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o64, k_tri_tiles<double>, threads, 0));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o32, k_tri_tiles<float>, threads, 0));
+  int per_sm = o64 < o32 ? o64 : o32;
+  if (per_sm > tiles_per_sm) per_sm = tiles_per_sm;
+  BN_REQUIRE(per_sm > 0, BN_ERR_CUDA, "IC(0): tiled sweep block does not fit");
+  tl.threads = threads;
+  tl.ntiles = sms * per_sm;
+  tl.rows_per_tile = n > 0 ? (n + tl.ntiles - 1) / tl.ntiles : 1;
+  const int R = tl.rows_per_tile;
+  tl.tile_steps.alloc(tl.ntiles, s);
+  tl.tile_steps.zero();  // empty tiles: [0, 0)
+  tl.imask.alloc(n > 0 ? n : 1, s);
+  tl.nsteps = 0;
+  if (n == 0) {
+    tl.steps.alloc(1, s);
+    return;
+  }
+  const int g = grid_for(n, 256);
+  DBuf<int> lev(n, s), head(n, s), starts(n, s), nsel(1, s);
+  BN_LAUNCH(k_pos_level, g, 256, 0, s, dptr.p, nlevels, n, lev.p);
+  BN_LAUNCH(k_step_heads, g, 256, 0, s, rows, lev.p, n, R, tl.ntiles, forward ? 1 : 0, head.p);
+  DBuf<int> pos(n, s);
+  BN_LAUNCH(k_iota_i, g, 256, 0, s, pos.p, n);
+  size_t tmp = 0;
+  BN_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, pos.p, head.p, starts.p, nsel.p, n, s));
+  {
+    DBuf<unsigned char> t(tmp, s);
+    BN_CUDA(cub::DeviceSelect::Flagged(t.p, tmp, pos.p, head.p, starts.p, nsel.p, n, s));
+  }
+  const int ns = read_scalar(nsel.p, s);
+  tl.nsteps = ns;
+  DBuf<int> stile(ns, s), sids(ns, s), stile2(ns, s), sids2(ns, s);
+  BN_LAUNCH(k_step_tiles, grid_for(ns, 256), 256, 0, s, starts.p, ns, rows, R, tl.ntiles,
+            forward ? 1 : 0, stile.p, sids.p);
+  int eb = 1;
+  while ((1 << eb) <= tl.ntiles) eb++;
+  tmp = 0;
+  BN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, stile.p, stile2.p, sids.p, sids2.p, ns, 0,
+                                          eb, s));
+  {
+    DBuf<unsigned char> t(tmp, s);
+    BN_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, stile.p, stile2.p, sids.p, sids2.p, ns, 0,
+                                            eb, s));
+  }
+  tl.steps.alloc(ns, s);
+  BN_LAUNCH(k_step_ranges, grid_for(ns, 256), 256, 0, s, sids2.p, starts.p, ns, n, stile2.p,
+            tl.steps.p, tl.tile_steps.p);
+  BN_LAUNCH(k_tile_mask, g, 256, 0, s, tia, tja, rows, n, R, tl.imask.p);
+  BN_CUDA(cudaStreamSynchronize(s));
 }
 
 template <class T>
@@ -866,13 +1093,20 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   } else {
     fv = fval32.p; fd = fdiag32.p; bv = bval32.p; bd = bdiag32.p;
   }
+  if (mode == kSweepTiles) {
+    if (n == 0) return;
+    BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
+    run_tri_tiles<T>(tf, fia.p, vfja.p, fv, fd, vorder.p, b, y, x, wait.ctl(WT_IC_FWD), s);
+    run_tri_tiles<T>(tb, bia.p, vbja.p, bv, bd, vborder.p, y, x, nullptr, wait.ctl(WT_IC_BWD), s);
+    return;
+  }
   if (mode == kSweepFlags) {
     if (n == 0) return;
     BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
     run_tri_flags<T>(n_fchunk, d_fchunk.p, blocks_per_sm, fia.p, vfja.p, fv, fd, vorder.p, b, y,
-                     x, err.p, s);
+                     x, wait.ctl(WT_IC_FWD), s);
     run_tri_flags<T>(n_bchunk, d_bchunk.p, blocks_per_sm, bia.p, vbja.p, bv, bd, vborder.p, y, x,
-                     nullptr, err.p, s);
+                     nullptr, wait.ctl(WT_IC_BWD), s);
     return;
   }
   if (mode == kSweepCoop) {
@@ -887,11 +1121,40 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
 template void IChol::solve<double>(const double*, double*, double*, cudaStream_t);
 template void IChol::solve<float>(const float*, float*, float*, cudaStream_t);
 
-int IChol::take_error(cudaStream_t s) {
-  if (!err.p) return 0;
-  int e = read_scalar(err.p, s);
-  if (e) err.zero();
-  return e ? BN_ERR_SPIN : 0;
+void IChol::check_waits(cudaStream_t s) {
+  if (!wait.rec.p) return;
+  std::string msg;
+  if (wait.take(s, &msg)) throw Error(BN_ERR_SPIN, "IC(0) solve: " + msg);
+}
+
+unsigned long long WaitRecord::default_limit_ns() {
+  // A legitimate wait lasts at most the time the grid's other warps take
+  // for their current chunks (milliseconds on the largest networks); a
+  // second is far above that and still ends a stuck sweep promptly.
+  static const unsigned long long v = [] {
+    const char* e = getenv("BN_WAIT_LIMIT_MS");
+    const double ms = e ? atof(e) : 1000.0;
+    return (unsigned long long)((ms > 0.01 ? ms : 0.01) * 1e6);
+  }();
+  return v;
+}
+
+int WaitRecord::take(cudaStream_t s, std::string* msg) {
+  int h[kWaitWords];
+  rec.download(h, kWaitWords);
+  BN_CUDA(cudaStreamSynchronize(s));
+  if (h[0] == 0) return 0;
+  rec.zero();
+  static const char* names[] = {"?", "forward IC(0) sweep", "backward IC(0) sweep",
+                                "ordered Gauss-Seidel sweep", "wait self-test"};
+  const int tag = (h[1] >= 1 && h[1] <= 4) ? h[1] : 0;
+  char buf[256];
+  snprintf(buf, sizeof buf,
+           "a bounded dependency wait ran out (%s: row %d waited %.3f ms for row %d; the "
+           "sweep was abandoned)",
+           names[tag], h[2], h[4] * 1e-3, h[3]);
+  if (msg) *msg = buf;
+  return BN_ERR_SPIN;
 }
 
 int IChol::blocks_from_env() {
@@ -899,12 +1162,80 @@ int IChol::blocks_from_env() {
   return v ? atoi(v) : 2;  // 2 blocks of 256 per SM measured fastest on the 20M network
 }
 
+// The give-up path of the bounded waits, on demand: the forward sweep
+// kernel over an n-row chain (row t depends on row t-1) whose first row is
+// left out of the schedule, so row 1 waits for a value that nothing
+// publishes.  Its wait runs out after limit_ns, raises the abort word, and
+// rows 2..n-1 end at once (they see NaN or the abort word).  Throws the
+// sweep's BN_ERR_SPIN; *elapsed_ms receives the launch's device time.
+void wait_selftest(int n, double limit_ms, double* elapsed_ms, cudaStream_t s) {
+  BN_REQUIRE(n >= 2 && n <= (1 << 20), BN_ERR_ARG, "wait self-test: 2 <= n <= 2^20 rows");
+  BN_REQUIRE(limit_ms > 0.0 && limit_ms <= 10000.0, BN_ERR_ARG,
+             "wait self-test: 0 < limit <= 10000 ms");
+  std::vector<int> ia(n + 1), ja(n - 1), rows(n);
+  std::vector<double> val(n - 1, 0.5), diag(n, 1.0), in(n, 1.0);
+  std::vector<int2> chunks;
+  ia[0] = 0;
+  for (int t = 0; t < n; t++) {
+    ia[t + 1] = ia[t] + (t > 0);
+    if (t > 0) ja[t - 1] = t - 1;
+    rows[t] = t;
+    if (t > 0) chunks.push_back(make_int2(t, t + 1));  // row 0 is never computed
+  }
+  DBuf<int> dia(n + 1, s), dja(n - 1, s), drows(n, s);
+  DBuf<double> dval(n - 1, s), ddiag(n, s), din(n, s), dout(n, s);
+  DBuf<int2> dch(chunks.size(), s);
+  dia.upload(ia.data(), n + 1);
+  dja.upload(ja.data(), n - 1);
+  drows.upload(rows.data(), n);
+  dval.upload(val.data(), n - 1);
+  ddiag.upload(diag.data(), n);
+  din.upload(in.data(), n);
+  dch.upload(chunks.data(), chunks.size());
+  dout.fill_bytes(0xff);
+  WaitRecord wait;
+  wait.init(s);
+  wait.limit_ns = (unsigned long long)(limit_ms * 1e6);
+  cudaEvent_t e0, e1;
+  BN_CUDA(cudaEventCreate(&e0));
+  BN_CUDA(cudaEventCreate(&e1));
+  BN_CUDA(cudaEventRecord(e0, s));
+  run_tri_flags<double>((int)chunks.size(), dch.p, 2, dia.p, dja.p, dval.p, ddiag.p, drows.p,
+                        din.p, dout.p, nullptr, wait.ctl(WT_SELFTEST), s);
+  BN_CUDA(cudaEventRecord(e1, s));
+  BN_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (elapsed_ms) *elapsed_ms = ms;
+  std::string msg;
+  if (wait.take(s, &msg)) throw Error(BN_ERR_SPIN, "wait self-test: " + msg);
+}
+
 int IChol::mode_from_env() {
   const char* v = getenv("BN_IC_MODE");
-  if (!v) return kSweepFlags;
+  if (!v) return kSweepTiles;
   if (!strcmp(v, "levels")) return kSweepLevels;
   if (!strcmp(v, "coop")) return kSweepCoop;
-  return kSweepFlags;
+  if (!strcmp(v, "flags")) return kSweepFlags;
+  return kSweepTiles;
 }
 
 }  // namespace bn
+
+// See include/amg_b200.h for the contract.
+BN_API int amg_debug_wait_timeout(int n, double limit_ms, double* elapsed_ms) {
+  using namespace bn;
+  try {
+    wait_selftest(n, limit_ms, elapsed_ms, cudaStreamPerThread);
+    set_last_error(BN_OK, "");
+    return BN_OK;
+  } catch (const Error& e) {
+    set_last_error(e.code, e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(BN_ERR_CUDA, e.what());
+    return BN_ERR_CUDA;
+  }
+}

@@ -1,6 +1,7 @@
 // IC(0) factor and level-scheduled triangular solves.
 #pragma once
 #include "internal.cuh"
+#include "flags.cuh"
 
 namespace bn {
 
@@ -26,13 +27,27 @@ struct IChol {
   DBuf<int4> d_cfseg, d_cbseg;  // cooperative schedules (narrow = 1024 rows)
   int n_cfseg = 0, n_cbseg = 0;
   // sweep form: level launches, one cooperative launch with a grid barrier
-  // per level, or the sync-free form (default; BN_IC_MODE=levels|coop|flags)
-  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2 };
+  // per level, the sync-free form over 32-row chunks, or the tiled form
+  // (default; BN_IC_MODE=levels|coop|flags|tiles)
+  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3 };
   int mode = mode_from_env();
   int blocks_per_sm = blocks_from_env();  // sync-free grid: blocks per SM (0: occupancy)
-  DBuf<int> err;                // sync-free form: a wait ran out
+  WaitRecord wait;              // sync-free and tiled forms: bounded waits and their record
   DBuf<int2> d_fchunk, d_bchunk;  // sync-free form: 32-row chunks within levels
   int n_fchunk = 0, n_bchunk = 0;
+  // tiled form: tile q holds the rows of index range [q R, (q+1) R) (the
+  // forward sweep; the backward sweep takes the tiles in reverse); a step
+  // is the tile's rows of one level, a contiguous range of the level-ordered
+  // layout.  tile_steps[q] = [first step, end step), steps[k] = [first
+  // position, end position).  imask[t]: bit q set when entry q of row t
+  // depends on a row of the same tile (read from the block's own earlier
+  // steps); other entries poll their dependency.
+  struct Tiles {
+    int ntiles = 0, rows_per_tile = 0, threads = 0, nsteps = 0;
+    DBuf<int2> tile_steps, steps;
+    DBuf<unsigned> imask;
+  };
+  Tiles tf, tb;
   DBuf<int> fia, fja, fsrc; // forward rows (level order)
   DBuf<int> bia, bja, bsrc; // backward rows (reverse level order)
   // vector indices used by the solves: the rows/columns above mapped into
@@ -49,9 +64,12 @@ struct IChol {
   // x = (L L^T)^{-1} b ; y is scratch (n)
   template <class T>
   void solve(const T* b, T* y, T* x, cudaStream_t s);
-  int take_error(cudaStream_t s);               // BN_ERR_SPIN if a wait ran out (then cleared)
+  // throws BN_ERR_SPIN (with the record's row, dependency and time) if a
+  // wait of the last sweeps ran out; the record is cleared
+  void check_waits(cudaStream_t s);
   static int mode_from_env();
   static int blocks_from_env();
+  void build_tiles(bool forward, cudaStream_t s);
   int launches_per_solve() const { return (int)(fseg.size() + bseg.size()); }
 };
 

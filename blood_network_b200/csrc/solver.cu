@@ -975,8 +975,7 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   reduce_partials(part1.p, kRedBlocks, sc.p + SC_RR, s);   // r.r
   BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
   BN_CUDA(cudaStreamSynchronize(s));
-  int icerr = ic.take_error(s);
-  if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+  ic.check_waits(s);
   double bnorm = sqrt(h_sc[SC_BB]);
   if (bnorm == 0.0) bnorm = 1.0;
   const double rz0 = h_sc[SC_RZ];
@@ -1003,8 +1002,7 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
     pcg_scalars(sc.p, flexible ? 1 : 0, s);
     BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
     BN_CUDA(cudaStreamSynchronize(s));
-    icerr = ic.take_error(s);
-    if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+    ic.check_waits(s);
     const double rz_new = h_sc[SC_RZ];  // rotated: SC_RZ now holds r_{k+1}.z_{k+1}
     rnorm = sqrt(h_sc[SC_RR]);
     bn_rel = sqrt(rz_new / rz0);
@@ -1119,8 +1117,7 @@ int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double*
   BN_CUDA(cudaMemcpyAsync(S_(RZ0), S_(RZ), sizeof(double) * nseg, cudaMemcpyDeviceToDevice, s));
   BN_LAUNCH(k_seg_start, grid_for(nseg, 256), 256, 0, s, S_(RZ), nseg, active, iters, flag + 1);
   int nact = read_scalar(flag + 1, s);
-  int icerr = ic.take_error(s);
-  if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+  ic.check_waits(s);
   const int relres = (opt.stop == AMG_STOP_RELRES) ? 1 : 0;
   int iter = 0;
   for (iter = 1; iter <= maxiter && nact > 0; iter++) {
@@ -1137,8 +1134,7 @@ int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double*
              nseg, flexible ? 1 : 0, relres, tol, iter, flag + 1, s);
     seg_update_p(p.p, z.p, seg.p, S_(BETA), n0, s);
     nact = read_scalar(flag + 1, s);
-    icerr = ic.take_error(s);
-    if (icerr) throw Error(icerr, "IC(0) solve: a bounded dependency wait ran out");
+    ic.check_waits(s);
   }
   // true residual per segment
   spmv<double>(SPMV_RES, A, x.p, b.p, ap.p, s);
@@ -1506,8 +1502,7 @@ BN_API int amg_solver_precond(void* h, const double* g, double* xo) {
     bn::vpermute<double>(px.p, S->lv[0]->perm.p, n, dx.p, true, S->s);
     dx.download(xo, n);
     BN_CUDA(cudaStreamSynchronize(S->s));
-    int e = S->ic.take_error(S->s);
-    BN_REQUIRE(e == 0, e, "IC(0) solve: a bounded dependency wait ran out");
+    S->ic.check_waits(S->s);
     return 0;
   }, bn::BN_ERR_CUDA);
 }

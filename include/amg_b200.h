@@ -387,6 +387,19 @@ int amg_network_adjoint_device(void* solver, const amg_network_system* sys, int 
                                const double* d_dLdp, double tol, int maxiter, double* d_lambda,
                                double* d_dLdg, int* iterations);
 
+/* amg_debug_wait_timeout: no counterpart in the reference (its solver has
+ * no waits).  Exercises the give-up path of the sync-free sweeps' bounded
+ * waits: runs the IC(0) forward-sweep kernel on an n-row chain (row t
+ * depends on row t-1; 2 <= n <= 2^20) whose first row is left out of the
+ * schedule, so row 1 waits for a value that is never published.  That wait
+ * runs out after limit_ms (0 < limit_ms <= 10000), raises the sweep's abort
+ * word, and every other waiting row ends at once.  The expected result is
+ * AMG_ERR_SPIN, with the wait record (sweep, row, dependency, time waited)
+ * in amg_solver_last_error(); *elapsed_ms (may be NULL) receives the
+ * launch's device time, about limit_ms.  The device stays usable.  Any
+ * other return means the give-up path is broken. */
+int amg_debug_wait_timeout(int n, double limit_ms, double* elapsed_ms);
+
 /* ichol_solve_noalloc: no counterpart in the reference.  Solves L L^T x = b
  * for an IC(0) factor already in device memory (0-based CSR d_ia[n+1],
  * d_ja/d_val[nnz] as ichol_compute returns it, lower triangle, diagonal

@@ -1,3 +1,4 @@
+import faulthandler
 import os
 import sys
 
@@ -12,6 +13,24 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+# A test that runs past BN_TEST_LIMIT_S seconds (default 300; the whole GPU
+# suite takes about a minute) dumps every thread's stack to stderr and ends
+# the run, so a stall shows where it happened instead of using up the
+# caller's time limit.
+_TEST_LIMIT_S = float(os.environ.get("BN_TEST_LIMIT_S", "300"))
+
+
+@pytest.hookimpl(hookwrapper=True)
+def pytest_runtest_protocol(item, nextitem):
+    if _TEST_LIMIT_S > 0:
+        faulthandler.dump_traceback_later(_TEST_LIMIT_S, exit=True, file=sys.__stderr__)
+    try:
+        yield
+    finally:
+        if _TEST_LIMIT_S > 0:
+            faulthandler.cancel_dump_traceback_later()
 
 
 @pytest.fixture(scope="session")

@@ -55,15 +55,31 @@ def _tie_frac(i):
     return (x >> np.uint64(1)).astype(np.float64) * (1.0 / 2147483648.0)
 
 
-def rs_first_pass(n, Sia, Sja, rs_quirk):
+def reference_draws(n):
+    """rand() after srand(12345): the C library's own generator (the
+    sequence the reference's HMIS weights use, rs_classical.c:542-551)."""
+    libc = C.CDLL(None)
+    libc.srand(12345)
+    return np.array([libc.rand() for _ in range(n)], np.float64)
+
+
+RAND_MAX = 2147483647.0
+
+
+def rs_first_pass(n, Sia, Sja, rs_quirk, hmis=False):
     """The device's parallel RS first pass, restated: rounds select undecided
     local maxima of lambda + tie over G = S u S^T; undecided points with a
-    strong C become F; each new F adds 1 to its undecided strong dependencies."""
+    strong C become F; each new F adds 1 to its undecided strong dependencies.
+    The tie is the reference HMIS's rand()/RAND_MAX for HMIS, a hash of the
+    index for RS."""
     rows = np.repeat(np.arange(n), np.diff(Sia))
     lam = np.bincount(Sja, minlength=n).astype(np.int64)
     if rs_quirk:
         lam[0] = 0
-    w = lam.astype(np.float64) + _tie_frac(np.arange(n))
+    if hmis:
+        w = lam.astype(np.float64) + reference_draws(n) / RAND_MAX
+    else:
+        w = lam.astype(np.float64) + _tie_frac(np.arange(n))
     gi = np.r_[rows, Sja]   # G edges (i, j): S rows and S^T rows
     gj = np.r_[Sja, rows]
     cf = np.zeros(n, np.int32)
@@ -158,7 +174,7 @@ def test_hub_splits(oracle, theta):
         assert a.tobytes() == b.tobytes()
     # HMIS and RS first passes
     for name, quirk in (("hmis", False), ("rs", True)):
-        want = rs_first_pass(n, S[0], S[1], quirk)
+        want = rs_first_pass(n, S[0], S[1], quirk, hmis=(name == "hmis"))
         cf = np.zeros(n, np.int32)
         nc = C.c_int()
         if name == "hmis":
@@ -167,6 +183,24 @@ def test_hub_splits(oracle, theta):
             lib.rs_coarsening(C.byref(_dcsr(n, *S)), ml, amg._p(cf), C.byref(nc))
         assert np.array_equal(cf, want), name
         assert nc.value == int((want == 1).sum())
+
+
+@pytest.mark.gpu
+def test_hmis_leaves_the_callers_rand_state():
+    """The reference's HMIS first pass never reseeds the C library's
+    generator; the device HMIS draws its weights from a private copy."""
+    lib = amg.load_library()
+    n, ia, ja, val = hub_matrix(side=30, hubs=(200,), weak_hubs=())
+    S, ml = _strength(lib, n, (ia, ja, val), 0.5)
+    libc = C.CDLL(None)
+    libc.srand(777)
+    want = [libc.rand() for _ in range(3)]
+    libc.srand(777)
+    cf = np.zeros(n, np.int32)
+    nc = C.c_int()
+    lib.hmis_coarsening(C.byref(_dcsr(n, *S)), amg._p(cf), C.byref(nc))
+    assert nc.value > 0
+    assert [libc.rand() for _ in range(3)] == want
 
 
 @pytest.mark.gpu
