@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <atomic>
 #include <string>
 #include <stdexcept>
 #include <vector>
@@ -53,8 +54,9 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
   do { if (!(cond)) throw ::bn::Error((code), (msg)); } while (0)
 
 // Launch accounting: every kernel launch in this library goes through
-// BN_LAUNCH so the host can report how many of its kernels ran.
-extern unsigned long long g_launch_count;
+// BN_LAUNCH so the host can report how many of its kernels ran (atomic:
+// entry points may be called from several host threads).
+extern std::atomic<unsigned long long> g_launch_count;
 #define BN_LAUNCH(kernel, grid, block, smem, stream, ...)                 \
   do {                                                                     \
     ::bn::g_launch_count++;                                                \

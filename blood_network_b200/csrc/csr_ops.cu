@@ -16,7 +16,7 @@
 
 namespace bn {
 
-unsigned long long g_launch_count = 0;
+std::atomic<unsigned long long> g_launch_count{0};
 
 bool trace_on() {
   static int on = -1;

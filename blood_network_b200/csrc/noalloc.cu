@@ -19,6 +19,8 @@
 #include "common.cuh"
 #include "../../include/amg_b200.h"
 
+#include <cuda.h>
+
 #include <mutex>
 
 namespace bn {
@@ -31,9 +33,32 @@ static __device__ __align__(256) double g_ichol_scratch[2 * kNoAllocMaxRows];
 
 // Device address of g_ichol_scratch per device, looked up once per device
 // with that device current (in host code the symbol is only a stand-in, not a
-// device address).
-static double* s_scratch[kNoAllocMaxDevices] = {nullptr};
+// device address), together with the context it belongs to: after a
+// cudaDeviceReset the device gets a new primary context in which the array
+// has a new address, so a changed context triggers a new lookup.
+struct ScratchAddr {
+  CUcontext ctx = nullptr;
+  double* p = nullptr;
+};
+static ScratchAddr s_scratch[kNoAllocMaxDevices];
 static std::mutex s_scratch_mutex;
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link-time
+// dependency on the driver library)
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+static CUcontext current_context() {
+  static CtxGetCurrentFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (CtxGetCurrentFn)f;
+  }();
+  CUcontext c = nullptr;
+  if (fn) fn(&c);
+  return c;
+}
 
 __global__ void __launch_bounds__(1024)
 k_ichol_solve_static(int n, const int* __restrict__ ia, const int* __restrict__ ja,
@@ -77,13 +102,16 @@ k_ichol_solve_static(int n, const int* __restrict__ ia, const int* __restrict__ 
 static int scratch_for_device(int dev, double** out) {
   if (dev < 0 || dev >= kNoAllocMaxDevices) return BN_ERR_ARG;
   std::lock_guard<std::mutex> lock(s_scratch_mutex);
-  if (!s_scratch[dev]) {
+  ScratchAddr& a = s_scratch[dev];
+  const CUcontext ctx = current_context();
+  if (!a.p || ctx != a.ctx) {
     double* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void**)&p, g_ichol_scratch);
     if (e != cudaSuccess || !p) return BN_ERR_CUDA;
-    s_scratch[dev] = p;
+    a.p = p;
+    a.ctx = current_context();  // the lookup made the primary context current
   }
-  *out = s_scratch[dev];
+  *out = a.p;
   return BN_OK;
 }
 
