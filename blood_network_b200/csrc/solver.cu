@@ -450,6 +450,85 @@ __global__ void k_iota_perm(int* __restrict__ a, int n) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) a[r] = r;
 }
 
+// ---- split of Ap by colour class (Level::AL / Level::AU)
+__global__ void k_row_class_start(const int* __restrict__ cptr, int ncls, int n,
+                                  int* __restrict__ cs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int lo = 0, hi = ncls - 1;  // last class starting at or before row i
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cptr[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    cs[i] = cptr[lo];
+  }
+}
+__global__ void k_split_count(const int* __restrict__ ia, const int* __restrict__ ja,
+                              const int* __restrict__ cs, int n, int* __restrict__ cl,
+                              int* __restrict__ cu) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int nlow = 0, nall = 0;
+    for (int k = ia[i]; k < ia[i + 1]; k++) {
+      const int j = ja[k];
+      nlow += (j < cs[i] || j == i);
+      nall++;
+    }
+    cl[i] = nlow;
+    cu[i] = nall - nlow;
+  }
+}
+__global__ void k_split_fill(const int* __restrict__ ia, const int* __restrict__ ja,
+                             const double* __restrict__ a, const int* __restrict__ cs, int n,
+                             const int* __restrict__ lia, int* __restrict__ lja,
+                             double* __restrict__ la, const int* __restrict__ uia,
+                             int* __restrict__ uja, double* __restrict__ ua) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int pl = lia[i], pu = uia[i];
+    for (int k = ia[i]; k < ia[i + 1]; k++) {
+      const int j = ja[k];
+      if (j < cs[i] || j == i) {
+        lja[pl] = j;
+        la[pl++] = a[k];
+      } else {
+        uja[pu] = j;
+        ua[pu++] = -a[k];
+      }
+    }
+  }
+}
+
+// AL / AU of a coloured level (entries keep their order within each part)
+void Solver::build_split(Level& L) {
+  const CSR& A = L.Ap;
+  const int n = A.n;
+  const int ncls = (int)L.cptr.size() - 1;
+  const int g = grid_for(n, 256);
+  DBuf<int> cs(n, s), cl((size_t)n + 1, s), cu((size_t)n + 1, s);
+  cl.zero();
+  cu.zero();
+  BN_LAUNCH(k_row_class_start, g, 256, 0, s, L.d_cptr.p, ncls, n, cs.p);
+  BN_LAUNCH(k_split_count, g, 256, 0, s, A.ia.p, A.ja.p, cs.p, n, cl.p, cu.p);
+  const int nl = scan_counts(cl.p, n, s);
+  const int nu = scan_counts(cu.p, n, s);
+  L.AL.n = L.AU.n = n;
+  L.AL.m = L.AU.m = A.m;
+  L.AL.nnz = nl;
+  L.AU.nnz = nu;
+  L.AL.ia = std::move(cl);
+  L.AU.ia = std::move(cu);
+  L.AL.ja.alloc(nl > 0 ? nl : 1, s);
+  L.AL.val.alloc(nl > 0 ? nl : 1, s);
+  L.AU.ja.alloc(nu > 0 ? nu : 1, s);
+  L.AU.val.alloc(nu > 0 ? nu : 1, s);
+  BN_LAUNCH(k_split_fill, g, 256, 0, s, A.ia.p, A.ja.p, A.val.p, cs.p, n, L.AL.ia.p, L.AL.ja.p,
+            L.AL.val.p, L.AU.ia.p, L.AU.ja.p, L.AU.val.p);
+  analyze_rows(L.AL, L.layAL, s);
+  analyze_rows(L.AU, L.layAU, s);
+  order_tiles(n, L.perm.p, L.layAL, s);
+  order_tiles(n, L.perm.p, L.layAU, s);
+  L.split = true;
+}
+
 void permute_csr(const CSR& A, const int* perm, const int* cinv, CSR& B, cudaStream_t s) {
   const int n = A.n;
   DBuf<int> cnt((size_t)n + 1, s);
@@ -537,6 +616,14 @@ void Solver::build_solve_layout() {
           fprintf(stderr, "[bn] L%d packed kernels: A %d (%d long rows)  P %d  R %d (%d long rows)\n",
                   l, (int)L.use_pkA, L.layA.nlong, (int)L.use_pkP, (int)L.use_pkR, L.layR.nlong);
       }
+      L.split = false;
+      L.AL = CSR();
+      L.AU = CSR();
+      if (coloured_level(l) && !(use_packed && L.use_pkA) && L.A.n > kSmallLevel &&
+          L.layA.nlong == 0) {
+        Phase ph3("split by class", s, l);
+        build_split(L);
+      }
       if (opt.smoother == SMOOTHER_JACOBI || coloured_level(l)) {
         L.dg.alloc(L.A.n, s);
         BN_LAUNCH(k_diag, grid_for(L.A.n, 256), 256, 0, s, L.Ap.ia.p, L.Ap.ja.p, L.Ap.val.p,
@@ -588,6 +675,14 @@ void Solver::prepare_f32() {
     L.A32.alloc(L.Ap.nnz > 0 ? L.Ap.nnz : 1, s);
     BN_LAUNCH(k_to_f32<float>, grid_for(L.Ap.nnz, 256), 256, 0, s, L.Ap.val.p, (size_t)L.Ap.nnz,
               L.A32.p);
+    if (L.split) {
+      L.AL32.alloc(L.AL.nnz > 0 ? L.AL.nnz : 1, s);
+      L.AU32.alloc(L.AU.nnz > 0 ? L.AU.nnz : 1, s);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.AL.nnz, 256), 256, 0, s, L.AL.val.p,
+                (size_t)L.AL.nnz, L.AL32.p);
+      BN_LAUNCH(k_to_f32<float>, grid_for(L.AU.nnz, 256), 256, 0, s, L.AU.val.p,
+                (size_t)L.AU.nnz, L.AU32.p);
+    }
     if (l < nl - 1) {
       L.P32.alloc(L.Pp.nnz > 0 ? L.Pp.nnz : 1, s);
       L.R32.alloc(L.Rp.nnz > 0 ? L.Rp.nnz : 1, s);
@@ -758,7 +853,7 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
 
 // backslash_rec (amg_cycle.c:180-212); xl is zero on entry
 template <class T>
-void Solver::backslash(int l, const T* bb, T* xl) {
+void Solver::backslash(int l, const T* bb, T* xl, bool zero_guess) {
   const int nl = (int)lv.size();
   if (l == nl - 1) {
     coarse.apply<T>(bb, xl, s);
@@ -770,8 +865,21 @@ void Solver::backslash(int l, const T* bb, T* xl) {
   T* rr = f64 ? (T*)L.r.p : (T*)L.r32.p;
   T* cb = f64 ? (T*)C.b.p : (T*)C.b32.p;
   T* cx = f64 ? (T*)C.x.p : (T*)C.x32.p;
-  { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
-  {
+  const bool split = zero_guess && L.split && opt.nu == 1 &&
+                     (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS);
+  if (split) {
+    // first sweep from x = 0 on AL (every class, Jacobi classes included,
+    // reads only earlier classes: in place), then r = b - A x = AU x
+    Phase ph("gs forward (split) + residual", s, l);
+    DevMat<T> AL = mat<T>(L.AL, &L.AL32, &L.layAL);
+    const int nseg = (int)L.cptr.size() - 1;
+    for (int c = 0; c < nseg; c++) {
+      const int r0 = L.cptr[c];
+      gs_color<T>(AL, nullptr, r0, L.cptr[c + 1] - r0, bb, xl, L.gs_group, s, L.clong[c]);
+    }
+    spmv<T>(SPMV_Y, mat<T>(L.AU, &L.AU32, &L.layAU), xl, nullptr, rr, s);
+  } else {
+    { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
     Phase ph("residual", s, l);
     if (use_packed && L.use_pkA)
       packed_apply<T>(PK_RES, pmat<T>(L.Ap, L.A32, L.pkA), 0, xl, bb, rr, nullptr, 0, s);
@@ -786,7 +894,7 @@ void Solver::backslash(int l, const T* bb, T* xl) {
       spmv<T>(SPMV_Y, mat<T>(L.Rp, &L.R32, &L.layR), rr, nullptr, cb, s);
   }
   if (l + 1 < nl - 1) vzero<T>(cx, C.A.n, s);
-  backslash<T>(l + 1, cb, cx);
+  backslash<T>(l + 1, cb, cx, true);
   if (use_packed && L.use_pkP)  // x += P ec
     packed_apply<T>(PK_ADD, pmat<T>(L.Pp, L.P32, L.pkP), 0, cx, nullptr, xl, nullptr, 0, s);
   else
@@ -834,7 +942,7 @@ void Solver::precond_t(const T* g, T* out) {
   T* CO = f64 ? (T*)corr.p : (T*)corrf.p;
   DevMat<T> As = own_solve ? mat<T>(Aownp, &Aown32, &layOwn) : mat<T>(lv[0]->Ap, &lv[0]->A32, &lv[0]->layA);
   vzero<T>(U1, n0, s);
-  { Phase ph("backslash", s); backslash<T>(0, g, U1); }
+  { Phase ph("backslash", s); backslash<T>(0, g, U1, true); }
   const bool fine_packed = use_packed && !own_solve && lv[0]->use_pkA && lv[0]->pkA.ranges() == 1;
   PackedMat<T> Ap0 = pmat<T>(lv[0]->Ap, lv[0]->A32, lv[0]->pkA);
   if (fine_packed) {
@@ -862,14 +970,16 @@ void Solver::precond_t(const T* g, T* out) {
 void Solver::vcycle_apply(const double* g, double* out) {
   const int n0 = lv[0]->A.n;
   vzero<double>(u1.p, n0, s);
-  backslash<double>(0, g, u1.p);
+  backslash<double>(0, g, u1.p, true);
   spmv<double>(SPMV_RES, mat<double>(lv[0]->Ap, nullptr, &lv[0]->layA), u1.p, g, r1.p, s);
   fwdslash<double>(0, r1.p, corr.p);
   vadd<double>(u1.p, corr.p, n0, out, s);
 }
 
 // amg_backslash (amg_cycle.c:180-215) at level l; x is the initial guess
-void Solver::backslash_at(int l, const double* b, double* x) { backslash<double>(l, b, x); }
+void Solver::backslash_at(int l, const double* b, double* x) {
+  backslash<double>(l, b, x, false);
+}
 
 // amg_fwdslash (amg_cycle.c:222-253) at level l with x as the initial guess:
 // r = b - A x, coarse correction from R r, x += P e, post-smoothing

@@ -47,6 +47,17 @@ struct Level {
   // which operators run on the packed kernels: those with rows longer than
   // kLongRow (hub rows); the row-group kernels are faster on the others
   bool use_pkA = false, use_pkP = false, use_pkR = false;
+  // Ap split by colour class for the first smoothing sweep from a zero
+  // guess (coloured levels on the row-group kernels): AL row i holds the
+  // entries of row i in earlier classes plus the diagonal, AU the other
+  // off-diagonal entries negated.  A forward sweep from x = 0 reads only
+  // AL (later classes are still zero), and afterwards b - A x = AU x (each
+  // row's own equation held when it was updated), so the sweep and the
+  // residual read A once instead of twice.
+  bool split = false;
+  CSR AL, AU;
+  DBuf<float> AL32, AU32;
+  RowLayout layAL, layAU;
   // work vectors
   DBuf<double> b, x, r;
   DBuf<float> b32, x32, r32;
@@ -100,7 +111,10 @@ struct Solver {
   const CSR& Asolve_p() const { return own_solve ? Aownp : lv[0]->Ap; }
   void build_solve_layout();
   template <class T> void smooth(int l, const T* bb, T* xl, bool forward);
-  template <class T> void backslash(int l, const T* bb, T* xl);
+  // zero_guess: xl holds zeros on entry (every call inside the
+  // preconditioner), which allows the split first sweep
+  template <class T> void backslash(int l, const T* bb, T* xl, bool zero_guess);
+  void build_split(Level& L);
   template <class T> void fwdslash(int l, const T* bb, T* xl);
   template <class T> void precond_t(const T* g, T* out);
   void precond(const double* g, double* out);  // z = M g (FP64 interface)

@@ -42,6 +42,7 @@ def ref_lib():
         lib.refdrv_precond_apply.argtypes = [vp, vp, vp]
         lib.refdrv_timed.argtypes = [i, i] + [vp] * 5 + [d, i, i, i, d, i, vp, vp]
         lib.refdrv_free.argtypes = [vp]
+        lib.refdrv_update.argtypes = [vp, i, i, vp, vp, vp]
         _ref = lib
     return _ref
 
@@ -74,6 +75,12 @@ class RefSolver:
         x = np.zeros(self.n)
         self.lib.refdrv_precond_apply(self.h, _P(g), _P(x))
         return x
+
+    def update(self, indptr, indices, data):
+        """amg_solver_update: new values on the same pattern."""
+        a = (np.ascontiguousarray(indptr, np.int32), np.ascontiguousarray(indices, np.int32),
+             np.ascontiguousarray(data, np.float64))
+        self.lib.refdrv_update(self.h, self.n, int(a[0][-1]), _P(a[0]), _P(a[1]), _P(a[2]))
 
     def level(self, k):
         sz = np.zeros(5, np.int32)

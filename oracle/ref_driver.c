@@ -115,6 +115,29 @@ void refdrv_ichol_copy(void* h, int* ia, int* ja, double* val) {
 }
 
 /* One application of the AMG+ichol preconditioner (amg_ichol_precond.c:51). */
+/* refdrv_update mirrors amg_solver_update (C_amg1/src/amg_wrapper.c:114-149):
+ * symmetrise the new values, amg_rebuild_values on the kept hierarchy, new
+ * fine-level ichol. */
+void refdrv_update(void* h, int n, int nnz, const int* ia, const int* ja, const double* val) {
+  refdrv* d = (refdrv*)h;
+  dcsr_mat a, at, sum;
+  dcsr_mat_alloc(&a, n, n, nnz);
+  memcpy(a.ia, ia, (size_t)(n + 1) * sizeof(int));
+  memcpy(a.ja, ja, (size_t)nnz * sizeof(int));
+  memcpy(a.val, val, (size_t)nnz * sizeof(double));
+  dcsr_mat_alloc(&at, n, n, nnz);
+  dcsr_transz(&a, NULL, &at);
+  dcsr_mat_add(&a, &at, &sum);
+  for (int k = 0; k < sum.nnz; k++) sum.val[k] *= 0.5;
+  dcsr_mat_free(&a);
+  dcsr_mat_free(&at);
+  ichol_free(&d->L);
+  dcsr_mat_free(&d->A);
+  d->A = sum;
+  amg_rebuild_values(&d->amg, &d->A);
+  ichol_compute(&d->A, &d->L);
+}
+
 void refdrv_precond_apply(void* h, const double* g, double* x) {
   refdrv* d = (refdrv*)h;
   amg_ichol_precond(&d->amg, &d->A, &d->L, g, x);

@@ -182,11 +182,44 @@ def test_vcycle_is_backslash_then_fwdslash(built):
     assert np.linalg.norm(b1 - A1 @ x2) < np.linalg.norm(b1 - A1 @ x1)
 
 
-def test_rebuild_and_free(built):
+def test_rebuild_and_free(built, oracle):
+    """amg_rebuild_values with changed values (every segment's conductance
+    scaled by U(0.8, 1.25)): every level's A and P bit-identical to the
+    reference's amg_rebuild_values (build_hierarchy.c:170-242) on the same
+    matrices; then the original values again restore the original levels."""
+    if not oracle.have_reference():
+        pytest.skip("reference library not built")
+    from blood_network_b200.network import assemble
     lib, net, d, A, _ = built
     before = [_host_csr(d.levels[k].A)[2].copy() for k in range(d.num_levels)]
-    lib.amg_rebuild_values(C.byref(d), C.byref(A))
+    rng = np.random.default_rng(7)
+    g2 = net.conductance * rng.uniform(0.8, 1.25, net.conductance.shape[0])
+    new = assemble(net.n_total, net.seg_u, net.seg_v, g2, net.boundary, net.p_boundary)
+    ia2, ja2, val2 = (np.ascontiguousarray(new.indptr), np.ascontiguousarray(new.indices),
+                      np.ascontiguousarray(new.data))
+    A2 = _dcsr(ia2, ja2, val2, net.n)
+    lib.amg_rebuild_values(C.byref(d), C.byref(A2))
     assert lib.amg_solver_last_status() == 0, lib.amg_solver_last_error()
+    r = oracle.RefSolver(net.n, net.indptr, net.indices, net.data, theta=0.25, min_size=500,
+                         coarsening=1)
+    r.update(ia2, ja2, val2)
+    try:
+        assert d.num_levels == r.num_levels
+        for k in range(d.num_levels):
+            want = r.level(k)
+            got = _host_csr(d.levels[k].A)
+            for j in range(3):
+                assert bits_equal(got[j], want["A"][j]), ("A", k, j)
+            if k < d.num_levels - 1:
+                gotp = _host_csr(d.levels[k].P)
+                for j in range(3):
+                    assert bits_equal(gotp[j], want["P"][j]), ("P", k, j)
+    finally:
+        r.close()
+    changed = sum(not bits_equal(_host_csr(d.levels[k].A)[2], before[k])
+                  for k in range(d.num_levels))
+    assert changed == d.num_levels
+    lib.amg_rebuild_values(C.byref(d), C.byref(A))
     for k in range(d.num_levels):
         assert bits_equal(_host_csr(d.levels[k].A)[2], before[k])
     tmp = amg.AmgData()

@@ -277,14 +277,17 @@ def test_symmetrize_huge_rows():
 
 
 @pytest.mark.gpu
-def test_spmv_dropins_with_a_long_row_among_short_rows():
-    """A row over 1024 entries inside a tile of short rows is summed once
-    (by the long-row kernel), in every SpMV form."""
+@pytest.mark.parametrize("long_len", [1100, 5000])
+def test_spmv_dropins_with_a_long_row_among_short_rows(oracle, long_len):
+    """The reference's abyvg / abyvam / abyvcs (sparse_ops.c:19-56) with a row
+    over 1024 entries among short rows: bit-identical to the oracle's
+    sequential row sums (the drop-ins sum every row in storage order, also
+    when the row's tile overflows the shared product buffer)."""
     rng = np.random.default_rng(11)
     n = 3000
     rows, cols = [], []
     for i in range(n):
-        c = rng.choice(n, 1100 if i == 100 else 3, replace=False)
+        c = rng.choice(n, long_len if i == 100 else 3, replace=False)
         rows += [i] * len(c)
         cols += list(c)
     import scipy.sparse as sp
@@ -292,19 +295,19 @@ def test_spmv_dropins_with_a_long_row_among_short_rows():
     A.sum_duplicates()
     A.sort_indices()
     ia, ja, val = (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data)
+    M = (ia, ja, val)
     lib = amg.load_library()
     x = rng.standard_normal(n)
     y0 = rng.standard_normal(n)
-    ax = A @ x
     y = np.zeros(n)
     lib.abyvg(amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(y))
-    assert np.allclose(y, ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+    assert y.tobytes() == oracle.orc_spmv(n, n, M, x, "y").tobytes()
     r = np.zeros(n)
     lib.abyvam(amg._p(y0), amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(r))
-    assert np.allclose(r, y0 - ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+    assert r.tobytes() == oracle.orc_spmv(n, n, M, x, "res", b=y0).tobytes()
     y2 = y0.copy()
     lib.abyvcs(amg._p(ia), amg._p(ja), amg._p(val), amg._p(x), n, amg._p(y2))
-    assert np.allclose(y2, y0 + ax, rtol=1e-12, atol=1e-12 * np.abs(ax).max())
+    assert y2.tobytes() == oracle.orc_spmv(n, n, M, x, "add", y0=y0).tobytes()
 
 
 @pytest.mark.gpu

@@ -213,6 +213,42 @@ def test_update_refreshes_values(net20k):
     assert relres(net20k.indptr, net20k.indices, a2, x, net20k.rhs) <= 1e-8
 
 
+def test_update_matches_the_reference_update(net20k, oracle):
+    """amg_solver_update with changed values (every segment's conductance
+    scaled by U(0.8, 1.25)) against the reference's own amg_solver_update
+    (amg_wrapper.c:114-149 -> amg_rebuild_values, build_hierarchy.c:170-242)
+    run on the same matrices: every level's A and P bit-identical, and the
+    same iteration count after the update."""
+    if not oracle.have_reference():
+        pytest.skip("reference library not built")
+    from blood_network_b200.network import assemble
+    n = net20k.n
+    rng = np.random.default_rng(5)
+    g2 = net20k.conductance * rng.uniform(0.8, 1.25, net20k.conductance.shape[0])
+    new = assemble(net20k.n_total, net20k.seg_u, net20k.seg_v, g2, net20k.boundary,
+                   net20k.p_boundary)
+    assert np.array_equal(new.indptr, net20k.indptr)
+    assert np.array_equal(new.indices, net20k.indices)
+    assert not np.array_equal(new.data, net20k.data)
+    s = _solver(n, net20k.indptr, net20k.indices, net20k.data)
+    r = oracle.RefSolver(n, net20k.indptr, net20k.indices, net20k.data, theta=0.25,
+                         min_size=500, coarsening=1)
+    s.update(new.indptr, new.indices, new.data)
+    r.update(new.indptr, new.indices, new.data)
+    assert s.num_levels == r.num_levels
+    for k in range(s.num_levels):
+        a, b = s.level(k), r.level(k)
+        for j in range(3):
+            assert bits_equal(a["A"][j], b["A"][j]), ("A", k, j)
+        if b["P"] is not None:
+            for j in range(3):
+                assert bits_equal(a["P"][j], b["P"][j]), ("P", k, j)
+    x, it = s.solve(new.rhs, tol=1e-8)
+    xr, itr = r.solve(new.rhs, tol=1e-8)
+    r.close()
+    assert it > 0 and abs(it - itr) <= 2, (it, itr)
+
+
 def test_two_matrix_mode(net20k, oracle):
     """amg_solver_set_matrix: hierarchy from Ap, IC(0) and PCG on A.  The
     three-stage preconditioner is only symmetric when both matrices agree, so
