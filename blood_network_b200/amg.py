@@ -45,7 +45,8 @@ class Stats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("relres", C.c_double),
                 ("bnorm_rel", C.c_double), ("setup_seconds", C.c_double),
                 ("solve_seconds", C.c_double), ("num_levels", C.c_int),
-                ("nnz_total", C.c_longlong), ("ichol_levels", C.c_int)]
+                ("nnz_total", C.c_longlong), ("ichol_levels", C.c_int),
+                ("device_loop", C.c_int)]
 
 
 class DcsrMat(C.Structure):

@@ -685,7 +685,9 @@ __global__ void k_seg_next(double* __restrict__ rz, const double* __restrict__ r
                            const double* __restrict__ bb, const double* __restrict__ rz0,
                            int* __restrict__ active, int* __restrict__ iters,
                            double* __restrict__ beta, int nseg, int flexible, int relres,
-                           double tol, int iter, int* nactive) {
+                           double tol, int iter, const int* __restrict__ iters_done,
+                           int* nactive) {
+  if (iters_done) iter = *iters_done + 1;  // device-driven loop: iterations done so far
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x) {
     if (!active[k]) { beta[k] = 0.0; continue; }
     const double b2 = bb[k] > 0.0 ? bb[k] : 1.0;
@@ -703,10 +705,10 @@ __global__ void k_seg_next(double* __restrict__ rz, const double* __restrict__ r
 void seg_next(double* rz, const double* rznew, const double* rzold_new, const double* rr,
               const double* bb, const double* rz0, int* active, int* iters, double* beta,
               int nseg, int flexible, int relres, double tol, int iter, int* nactive,
-              cudaStream_t s) {
+              cudaStream_t s, const int* iters_done) {
   if (nseg > 0)
     BN_LAUNCH(k_seg_next, grid_for(nseg, 256), 256, 0, s, rz, rznew, rzold_new, rr, bb, rz0,
-              active, iters, beta, nseg, flexible, relres, tol, iter, nactive);
+              active, iters, beta, nseg, flexible, relres, tol, iter, iters_done, nactive);
 }
 
 // Reduce a partial array into slot `dst` of the scalar block.

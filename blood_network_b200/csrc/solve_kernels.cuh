@@ -111,7 +111,7 @@ void seg_alpha(const double* rz, const double* pap, const int* active, int nseg,
 void seg_next(double* rz, const double* rznew, const double* rzold_new, const double* rr,
               const double* bb, const double* rz0, int* active, int* iters, double* beta,
               int nseg, int flexible, int relres, double tol, int iter, int* nactive,
-              cudaStream_t s);
+              cudaStream_t s, const int* iters_done = nullptr);
 void vxpby(double* p, const double* z, double b, int n, cudaStream_t s);   // p = z + b p
 void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
                    const double* sc, double* part, cudaStream_t s);

@@ -278,6 +278,8 @@ Solver::~Solver() {
 void Solver::drop_graphs() {
   for (auto& g : graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& g : loop)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
 }
 
 template <class T>
@@ -644,6 +646,7 @@ void Solver::build_solve_layout() {
 }
 
 void Solver::alloc_vectors() {
+  drop_graphs();  // the graphs hold the vectors' addresses
   const int nl = (int)lv.size();
   for (int l = 0; l < nl; l++) {
     Level& L = *lv[l];
@@ -662,6 +665,8 @@ void Solver::alloc_vectors() {
     for (auto* v : {&g32, &u1f, &r1f, &icyf, &icxf, &xxf, &r2f, &corrf}) v->alloc(n0, s);
   sc.alloc(SC_COUNT, s);
   sc.zero();
+  ctl.alloc(4, s);
+  ctl.zero();
   const int np = spmv_partials(n0, lay_solve().nlong);
   part0.alloc(kRedBlocks > np ? kRedBlocks : np, s);
   part1.alloc(kRedBlocks, s);
@@ -1024,7 +1029,7 @@ void l1_row_norms(const CSR& A, double* d_out, cudaStream_t s) {
 // z = M r for the PCG: r -> z (captured once per precision as a CUDA graph)
 void Solver::precond(const double* g, double* out) {
   const int mode = opt.precision == AMG_PREC_MIXED ? 1 : 0;
-  const bool use_graph = (g == r.p && out == z.p) && !trace_on();
+  const bool use_graph = (g == r.p && out == z.p) && !trace_on() && !capture_direct;
   if (use_graph && graph[mode]) {
     BN_CUDA(cudaGraphLaunch(graph[mode], s));
     g_launch_count += graph_kernels[mode];
@@ -1062,6 +1067,90 @@ void Solver::precond(const double* g, double* out) {
   g_launch_count += graph_kernels[mode];
 }
 
+// ------------------------------------------------------------ device loops
+// Stopping test of one PCG iteration on the device (the host loop's test):
+// ctl[0] iterations done, ctl[1] status (0 go on, 1 converged, 2 non-finite,
+// 3 maxiter reached), ctl[2] maxiter, ctl[3] 1 = true relative residual
+// test, else the reference's B-norm; sc[SC_TOL] the tolerance.
+constexpr int SC_TOL = 9;
+__global__ void k_pcg_check(const double* __restrict__ sc, int* ctl,
+                            cudaGraphConditionalHandle h) {
+  const int it = ++ctl[0];
+  const double rz_new = sc[SC_RZ];
+  const double rnorm = sqrt(sc[SC_RR]);
+  double bn = sqrt(sc[SC_BB]);
+  if (bn == 0.0) bn = 1.0;
+  int st = 0;
+  if (!isfinite(rz_new) || !isfinite(rnorm)) {
+    st = 2;
+  } else {
+    const double crit = ctl[3] ? rnorm / bn : sqrt(rz_new / sc[SC_RZ0]);
+    if (crit < sc[SC_TOL]) st = 1;
+    else if (it >= ctl[2]) st = 3;
+  }
+  ctl[1] = st;
+  cudaGraphSetConditional(h, st == 0 ? 1u : 0u);
+}
+// segmented loop: go on while a segment iterates and maxiter is not reached
+__global__ void k_seg_cond(const int* __restrict__ nactive, int* ctl,
+                           cudaGraphConditionalHandle h) {
+  const int it = ++ctl[0];
+  cudaGraphSetConditional(h, (*nactive > 0 && it < ctl[2]) ? 1u : 0u);
+}
+
+// Captures body() (the kernels of one iteration, ending with the kernel that
+// sets the loop condition) as the body of a conditional WHILE node; the
+// graph runs the body until the condition is cleared.  Returns null where
+// the driver does not support it (the caller keeps the host loop).
+template <class F>
+static cudaGraphExec_t build_loop_graph(cudaStream_t s, F&& body,
+                                        unsigned long long* body_kernels) {
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaGraphConditionalHandle h;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cudaGraphNode_t node;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess ||
+      (cp.conditional.handle = h, cp.conditional.type = cudaGraphCondTypeWhile,
+       cp.conditional.size = 1, cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess)) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return nullptr;
+  }
+  cudaGraph_t bg = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(s, bg, nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return nullptr;
+  }
+  const unsigned long long before = g_launch_count;
+  try {
+    body(h);
+  } catch (...) {
+    cudaGraph_t dummy;
+    cudaStreamEndCapture(s, &dummy);
+    cudaGraphDestroy(g);
+    g_launch_count = before;
+    throw;
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &out);
+  *body_kernels = g_launch_count - before;  // launched once per iteration on replay
+  g_launch_count = before;
+  cudaGraphExec_t ex = nullptr;
+  if (e != cudaSuccess || cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    ex = nullptr;
+  }
+  cudaGraphDestroy(g);
+  return ex;
+}
+
 // amg_pcg (amg_pcg.c:12-101) on device vectors.  FP64 throughout; the mixed
 // form uses the flexible (Polak-Ribiere) beta because its preconditioner is
 // not exactly symmetric.
@@ -1097,6 +1186,57 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   }
   int iter;
   int status = BN_OK;
+  const int mode = flexible ? 1 : 0;
+  stats.device_loop = 0;
+  if (loops_ok && print_level < 1 && !trace_on() && maxiter > 0 && !loop[mode]) {
+    loop[mode] = build_loop_graph(s, [&](cudaGraphConditionalHandle h) {
+      capture_direct = true;
+      int np = spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s, p.p, part0.p);
+      reduce_partials(part0.p, np, sc.p + SC_PAP, s);
+      pcg_update_xr(x.p, r.p, p.p, ap.p, n0, sc.p, part0.p, s);
+      reduce_partials(part0.p, kRedBlocks, sc.p + SC_RR, s);
+      if (flexible) {
+        dot_partials<double>(r.p, z.p, nullptr, n0, part1.p, nullptr, s);
+        reduce_partials(part1.p, kRedBlocks, sc.p + SC_RZOLD_NEW, s);
+      }
+      precond(r.p, z.p);
+      dot_partials<double>(r.p, z.p, nullptr, n0, part0.p, nullptr, s);
+      reduce_partials(part0.p, kRedBlocks, sc.p + SC_RZNEW, s);
+      pcg_scalars(sc.p, flexible ? 1 : 0, s);
+      g_launch_count++;
+      k_pcg_check<<<1, 1, 0, s>>>(sc.p, ctl.p, h);
+      BN_CUDA(cudaGetLastError());
+      pcg_update_p(p.p, z.p, n0, sc.p, s);
+      capture_direct = false;
+    }, &loop_kernels[mode]);
+    capture_direct = false;
+    if (!loop[mode]) loops_ok = false;
+  }
+  if (loops_ok && print_level < 1 && !trace_on() && maxiter > 0 && loop[mode]) {
+    // all iterations in one graph launch; the host reads the outcome once
+    const int hc[4] = {0, 0, maxiter, opt.stop == AMG_STOP_RELRES ? 1 : 0};
+    BN_CUDA(cudaMemcpyAsync(ctl.p, hc, sizeof hc, cudaMemcpyHostToDevice, s));
+    h_sc[0] = tol;
+    BN_CUDA(cudaMemcpyAsync(sc.p + SC_TOL, h_sc, sizeof(double), cudaMemcpyHostToDevice, s));
+    BN_CUDA(cudaMemcpyAsync(sc.p + SC_RZ0, sc.p + SC_RZ, sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    BN_CUDA(cudaGraphLaunch(loop[mode], s));
+    int hres[4];
+    BN_CUDA(cudaMemcpyAsync(hres, ctl.p, sizeof hres, cudaMemcpyDeviceToHost, s));
+    BN_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
+    BN_CUDA(cudaStreamSynchronize(s));
+    g_launch_count += (unsigned long long)hres[0] * loop_kernels[mode];
+    ic.check_waits(s);
+    stats.device_loop = 1;
+    rnorm = sqrt(h_sc[SC_RR]);
+    bn_rel = sqrt(h_sc[SC_RZ] / rz0);
+    if (hres[1] == 1) {
+      iter = hres[0];
+    } else {
+      iter = maxiter + 1;
+      if (hres[1] == 2) status = BN_ERR_NAN;
+    }
+  } else
   for (iter = 1; iter <= maxiter; iter++) {
     int np = spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s, p.p, part0.p);  // Ap, p.Ap
     reduce_partials(part0.p, np, sc.p + SC_PAP, s);
@@ -1230,6 +1370,47 @@ int Solver::pcg_segmented(int nseg, const int* d_ptr, const double* d_b, double*
   ic.check_waits(s);
   const int relres = (opt.stop == AMG_STOP_RELRES) ? 1 : 0;
   int iter = 0;
+  stats.device_loop = 0;
+  // one CUDA graph for all iterations: the body is one iteration for every
+  // segment, its last kernel keeps the loop going while a segment iterates
+  cudaGraphExec_t seg_loop = nullptr;
+  unsigned long long body_kernels = 0;
+  if (loops_ok && !trace_on() && maxiter > 0 && nact > 0) {
+    seg_loop = build_loop_graph(s, [&](cudaGraphConditionalHandle h) {
+      capture_direct = true;
+      spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s);
+      seg_dot(p.p, ap.p, d_ptr, inv0, nseg, S_(PAP), s);
+      seg_alpha(S_(RZ), S_(PAP), active, nseg, S_(ALPHA), s);
+      seg_update_xr(x.p, r.p, p.p, ap.p, seg.p, S_(ALPHA), n0, s);
+      if (relres) seg_dot(r.p, r.p, d_ptr, inv0, nseg, S_(RR), s);
+      if (flexible) seg_dot(r.p, z.p, d_ptr, inv0, nseg, S_(RZON), s);
+      precond(r.p, z.p);
+      seg_dot(r.p, z.p, d_ptr, inv0, nseg, S_(RZNEW), s);
+      BN_CUDA(cudaMemsetAsync(flag + 1, 0, sizeof(int), s));
+      seg_next(S_(RZ), S_(RZNEW), S_(RZON), S_(RR), S_(BB), S_(RZ0), active, iters, S_(BETA),
+               nseg, flexible ? 1 : 0, relres, tol, 0, flag + 1, s, ctl.p);
+      seg_update_p(p.p, z.p, seg.p, S_(BETA), n0, s);
+      g_launch_count++;
+      k_seg_cond<<<1, 1, 0, s>>>(flag + 1, ctl.p, h);
+      BN_CUDA(cudaGetLastError());
+      capture_direct = false;
+    }, &body_kernels);
+    capture_direct = false;
+    if (!seg_loop) loops_ok = false;
+  }
+  if (seg_loop) {
+    const int hc[4] = {0, 0, maxiter, 0};
+    BN_CUDA(cudaMemcpyAsync(ctl.p, hc, sizeof hc, cudaMemcpyHostToDevice, s));
+    BN_CUDA(cudaGraphLaunch(seg_loop, s));
+    int hres[4];
+    BN_CUDA(cudaMemcpyAsync(hres, ctl.p, sizeof hres, cudaMemcpyDeviceToHost, s));
+    BN_CUDA(cudaStreamSynchronize(s));
+    cudaGraphExecDestroy(seg_loop);
+    g_launch_count += (unsigned long long)hres[0] * body_kernels;
+    ic.check_waits(s);
+    stats.device_loop = 1;
+    iter = hres[0] + 1;
+  } else
   for (iter = 1; iter <= maxiter && nact > 0; iter++) {
     spmv<double>(SPMV_Y, A, p.p, nullptr, ap.p, s);
     seg_dot(p.p, ap.p, d_ptr, inv0, nseg, S_(PAP), s);

@@ -87,6 +87,14 @@ struct Solver {
   double* h_sc = nullptr;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   unsigned long long graph_kernels[2] = {0, 0};
+  // PCG iterations as one graph each (a conditional WHILE node whose body
+  // is one iteration, the stopping test evaluated on the device): [mode] for
+  // the single solve, seg_loop for the segmented one (rebuilt per call)
+  cudaGraphExec_t loop[2] = {nullptr, nullptr};
+  unsigned long long loop_kernels[2] = {0, 0};
+  DBuf<int> ctl;           // device loop state: [0] iterations done, [1] status, [2] maxiter
+  bool loops_ok = getenv("BN_HOST_LOOP") == nullptr;  // BN_HOST_LOOP=1: host-driven loops
+  bool capture_direct = false;  // precond(): emit the kernels (inside a loop capture)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   amg_solve_stats stats{};
 

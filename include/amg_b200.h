@@ -209,6 +209,9 @@ typedef struct {
   int num_levels;
   long long nnz_total;  /* sum of nnz over levels (operator complexity numerator) */
   int ichol_levels;     /* dependency levels of the fine IC(0) */
+  int device_loop;      /* 1: the last solve ran its PCG iterations as one CUDA
+                           graph with the stopping test on the device (no host
+                           round trip per iteration); 0: host-driven loop */
 } amg_solve_stats;
 
 int amg_solver_stats(void* handle, amg_solve_stats* out);
