@@ -776,6 +776,7 @@ def main():
     clocks.start()
     mx_dev, mx_its, mx_rel, launches = solve_steps(amg.PREC_MIXED, args.steps, args.warmup)
     clk = clocks.stop()
+    st_loop = st.device_loop  # the timed solves ran their iterations as one device loop
     x_mixed = d_x.clone()
     # accuracy: an FP64 solution to a much tighter true residual (untimed)
     lib.amg_solver_set_precision(h, amg.PREC_FP64)
@@ -801,16 +802,31 @@ def main():
     ms64 = C.c_double()
     ms32 = C.c_double()
     msgs = C.c_double()
+    ms_ic = C.c_double()
+    ms_split = C.c_double()
     lib.amg_solver_bench_kernel(h, 0, 0, reps, C.byref(ms64))
     lib.amg_solver_bench_kernel(h, 0, 1, reps, C.byref(ms32))
     lib.amg_solver_bench_kernel(h, 1, 1, reps, C.byref(msgs))
+    lib.amg_solver_bench_kernel(h, 3, 1, reps, C.byref(ms_ic))
+    lib.amg_solver_bench_kernel(h, 4, 1, reps, C.byref(ms_split))
     bytes64 = 12 * nnz + 4 * (n + 1) + 8 * n * 3      # val+ja, ia, x, b, r
     bytes32 = 8 * nnz + 4 * (n + 1) + 4 * n * 3
     bytes_gs32 = 8 * nnz + 4 * (n + 1) + 4 * n + 4 * n + 8 * n  # + row list, b, x r/w
+    # one FP32 IC(0) sweep: per strictly-lower entry its column and value
+    # (8 B); per row its entry pointer, vector index, diagonal, input and
+    # output (20 B)
+    nnz_l = (nnz - n) // 2
+    bytes_ic32 = 8 * nnz_l + 20 * n
+    # first sweep from zero + residual (split form): every entry once (AL,
+    # AU), two row pointer arrays, b read, x written and read, r written
+    bytes_split32 = 8 * nnz + 8 * (n + 1) + 4 * n * 4
     peak, peak_kind = peaks()
     gbs64 = bytes64 / (ms64.value * 1e-3) / 1e9
     gbs32 = bytes32 / (ms32.value * 1e-3) / 1e9
     gbs_gs = bytes_gs32 / (msgs.value * 1e-3) / 1e9
+    sweep_ms = ms_ic.value / 2.0  # an IC(0) solve is two sweeps
+    gbs_ic = bytes_ic32 / (sweep_ms * 1e-3) / 1e9
+    gbs_split = bytes_split32 / (ms_split.value * 1e-3) / 1e9
     traffic = None
     tf = os.path.join(HERE, "profiles", "spmv_fp64_traffic.json")
     if os.path.exists(tf):
@@ -887,6 +903,20 @@ def main():
             "accuracy": accuracy,
             "spmv": {"fp64_gbs": gbs64, "fp32_gbs": gbs32, "gs_sweep_fp32_gbs": gbs_gs,
                      "fp64_ms": ms64.value, "fp32_ms": ms32.value},
+            "kernels": {
+                "spmv_residual_fp64": {"ms": ms64.value, "bytes": bytes64, "gbs": gbs64,
+                                       "frac": gbs64 / peak},
+                "spmv_residual_fp32": {"ms": ms32.value, "bytes": bytes32, "gbs": gbs32,
+                                       "frac": gbs32 / peak},
+                "gs_sweep_fp32": {"ms": msgs.value, "bytes": bytes_gs32, "gbs": gbs_gs,
+                                  "frac": gbs_gs / peak},
+                "first_sweep_plus_residual_fp32": {"ms": ms_split.value,
+                                                   "bytes": bytes_split32, "gbs": gbs_split,
+                                                   "frac": gbs_split / peak},
+                "ic0_sweep_fp32": {"ms": sweep_ms, "bytes": bytes_ic32, "gbs": gbs_ic,
+                                   "frac": gbs_ic / peak,
+                                   "levels": st.ichol_levels}},
+            "device_loop": bool(st_loop),
             "roofline": {"bound": "hbm", "achieved": gbs64, "peak": peak, "unit": "GB/s",
                          "frac": gbs64 / peak, "traffic": traffic,
                          "kernel": "fine-level residual SpMV r=b-Ax, FP64 CSR",

@@ -1843,6 +1843,40 @@ BN_API int amg_solver_bench_kernel(void* h, int which, int precision, int reps, 
         case 2:
           S->precond(S->b.p, S->z.p);
           break;
+        case 4: {  // first sweep from zero + residual: split form where the level has it
+          if (S->lv.size() < 2) break;
+          bn::Level& L = L0;
+          const int nseg = (int)L.cptr.size() - 1;
+          if (!L.split) {
+            if (f32) S->smooth<float>(0, S->g32.p, S->u1f.p, true);
+            else S->smooth<double>(0, S->b.p, S->u1.p, true);
+            if (f32)
+              bn::spmv<float>(bn::SPMV_RES, S->mat<float>(L.Ap, &L.A32, &L.layA), S->u1f.p,
+                              S->g32.p, L.r32.p, S->s);
+            else
+              bn::spmv<double>(bn::SPMV_RES, S->mat<double>(L.Ap, nullptr, &L.layA), S->u1.p,
+                               S->b.p, L.r.p, S->s);
+            break;
+          }
+          for (int c = 0; c < nseg; c++) {
+            const int r0 = L.cptr[c];
+            if (f32)
+              bn::gs_color<float>(S->mat<float>(L.AL, &L.AL32, &L.layAL), nullptr, r0,
+                                  L.cptr[c + 1] - r0, S->g32.p, S->u1f.p, L.gs_group, S->s,
+                                  L.clong[c]);
+            else
+              bn::gs_color<double>(S->mat<double>(L.AL, nullptr, &L.layAL), nullptr, r0,
+                                   L.cptr[c + 1] - r0, S->b.p, S->u1.p, L.gs_group, S->s,
+                                   L.clong[c]);
+          }
+          if (f32)
+            bn::spmv<float>(bn::SPMV_Y, S->mat<float>(L.AU, &L.AU32, &L.layAU), S->u1f.p,
+                            nullptr, L.r32.p, S->s);
+          else
+            bn::spmv<double>(bn::SPMV_Y, S->mat<double>(L.AU, nullptr, &L.layAU), S->u1.p,
+                             nullptr, L.r.p, S->s);
+          break;
+        }
         default:
           if (f32) S->ic.solve<float>(S->g32.p, S->icyf.p, S->icxf.p, S->s);
           else S->ic.solve<double>(S->b.p, S->icy.p, S->icx.p, S->s);

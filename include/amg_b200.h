@@ -226,7 +226,9 @@ int amg_solver_level_copy(void* handle, int level, int* a_ia, int* a_ja, double*
 /* Times `reps` launches of one hot operation with CUDA events on the
  * solver's stream; *ms receives the mean milliseconds per launch.
  * which: 0 fine residual SpMV, 1 fine forward Gauss-Seidel sweep,
- * 2 preconditioner application, 3 IC(0) solve.  precision: 0 FP64, 1 FP32. */
+ * 2 preconditioner application, 3 IC(0) solve (two sweeps), 4 the fine
+ * level's first sweep from a zero guess plus the residual after it (the
+ * split form where the level has it).  precision: 0 FP64, 1 FP32. */
 int amg_solver_bench_kernel(void* handle, int which, int precision, int reps, double* ms);
 
 const char* amg_solver_last_error(void);
