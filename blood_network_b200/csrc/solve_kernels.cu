@@ -112,6 +112,177 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
   }
 }
 
+// ---- row tiles staged by the bulk-copy engine
+// The same tiles and summation order as k_spmv (ROWS = kRows), but each
+// tile's column indices and values reach shared memory by two 1D bulk
+// copies (cp.async.bulk, completion on an mbarrier) issued one tile ahead by
+// one thread, so the stream of A runs ahead of the arithmetic without
+// occupying the threads' load slots; the threads then gather x with
+// independent loads (indices already on chip) and sum each row in storage
+// order.  Blocks are persistent and double-buffer their tiles.  A bulk copy
+// moves 16-byte aligned pieces: the tile's range is rounded down to a 16-byte
+// boundary at its start, and the last 0-3 entries past the last boundary are
+// loaded by the threads.  Every mbarrier wait is bounded; one that runs out
+// records an error (g_stage_err) and the launch goes on.
+__device__ int g_stage_err = 0;
+constexpr int kStageCap = kTileNnz;  // entries staged per tile
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* b, unsigned bytes) {
+  asm volatile(
+      "{\n\t.reg .b64 st;\n\t"
+      "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(b)),
+      "r"(bytes)
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded: about a second at most (try_wait suspends the thread between polls)
+__device__ __forceinline__ void mbar_wait(unsigned long long* b, unsigned parity) {
+  for (int it = 0; it < (1 << 22); it++)
+    if (mbar_try_wait(b, parity)) return;
+  atomicExch(&g_stage_err, 1);
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* b) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(b))
+      : "memory");
+}
+
+template <class T, int MODE, bool DOT>
+__global__ void __launch_bounds__(kRows)
+k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
+              const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
+              const T* __restrict__ dw, double* __restrict__ partial, int skip_long,
+              const int* __restrict__ tiles) {
+  extern __shared__ __align__(16) unsigned char stage_mem[];
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ double red[kRows / 32];
+  constexpr int JB = ((kStageCap + 8) * 4 + 15) / 16 * 16;
+  constexpr int AB = ((kStageCap + 8) * (int)sizeof(T) + 15) / 16 * 16;
+  auto s_ja = [&](int q) { return (int*)(stage_mem + q * JB); };
+  auto s_a = [&](int q) { return (T*)(stage_mem + 2 * JB + q * AB); };
+  const int ntiles = (n + kRows - 1) / kRows;
+  auto tile_row = [&](int slot) { return (tiles ? tiles[slot] : slot) * kRows; };
+  // thread 0: stage the tile at `slot` into buffer q (or just arrive)
+  auto issue = [&](int q, int slot) {
+    const int r0 = tile_row(slot);
+    const int r1 = min(r0 + kRows, n);
+    const int e0 = ia[r0], e1 = ia[r1];
+    const int s0 = e0 & ~3, fl = e1 & ~3;
+    if (e1 - e0 <= kStageCap && fl > s0) {
+      const unsigned nb = (unsigned)(fl - s0);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive_tx(&bar[q], nb * 4u + nb * (unsigned)sizeof(T));
+      bulk_g2s(s_ja(q), ja + s0, nb * 4u, &bar[q]);
+      bulk_g2s(s_a(q), a + s0, nb * (unsigned)sizeof(T), &bar[q]);
+    } else {
+      mbar_arrive_tx(&bar[q], 0u);
+    }
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (int)blockIdx.x < ntiles) issue(0, blockIdx.x);
+  double dot = 0.0;
+  int q = 0;
+  for (int slot = blockIdx.x; slot < ntiles; slot += gridDim.x, q++) {
+    const int st = q & 1;
+    if (threadIdx.x == 0 && slot + (int)gridDim.x < ntiles) issue(st ^ 1, slot + gridDim.x);
+    const int r0 = tile_row(slot);
+    const int r1 = min(r0 + kRows, n);
+    const int e0 = ia[r0], e1 = ia[r1];
+    const int i = r0 + threadIdx.x;
+    int k0 = 0, k1 = 0;
+    T hold = T(0), hw = T(0);
+    if (i < r1) {
+      k0 = ia[i];
+      k1 = ia[i + 1];
+      if (MODE == SPMV_RES) hold = b[i];
+      if (MODE == SPMV_ADD) hold = y[i];
+      if (DOT) hw = dw[i];
+    }
+    const bool mine = i < r1 && !(skip_long && k1 - k0 > kLongRow);
+    mbar_wait(&bar[st], (unsigned)((q >> 1) & 1));
+    const int m = e1 - e0;
+    if (m <= kStageCap) {
+      const int s0 = e0 & ~3;
+      const int fl = max(e1 & ~3, s0);
+      int* sj = s_ja(st);
+      T* sa = s_a(st);
+      for (int k = fl + threadIdx.x; k < e1; k += kRows) {  // the last 0-3 entries
+        sj[k - s0] = ja[k];
+        sa[k - s0] = a[k];
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int k = e0 - s0 + threadIdx.x; k < e1 - s0; k += kRows)
+        sa[k] = dmul(sa[k], x[sj[k]]);
+      __syncthreads();
+      if (mine) {
+        for (int k = k0 - s0; k < k1 - s0; k++)
+          hold = (MODE == SPMV_RES) ? dsub(hold, sa[k]) : dadd(hold, sa[k]);
+      }
+    } else if (mine) {
+      for (int k = k0; k < k1; k++) {
+        const T p = dmul(a[k], x[ja[k]]);
+        hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
+      }
+    }
+    if (mine) {
+      y[i] = hold;
+      if (DOT) dot += (double)hw * (double)hold;
+    }
+    __syncthreads();  // both buffers' readers are done before the next issue
+  }
+  if (DOT) {
+    for (int off = 16; off > 0; off >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kRows / 32; w++) t += red[w];
+      partial[blockIdx.x] = t;
+    }
+  }
+}
+
+template <class T>
+constexpr int staged_smem_bytes() {
+  return 2 * (((kStageCap + 8) * 4 + 15) / 16 * 16) +
+         2 * (((kStageCap + 8) * (int)sizeof(T) + 15) / 16 * 16);
+}
+
+int take_stage_error() {
+  int e = 0;
+  BN_CUDA(cudaMemcpyFromSymbol(&e, g_stage_err, sizeof(int)));
+  if (e) {
+    const int z = 0;
+    BN_CUDA(cudaMemcpyToSymbol(g_stage_err, &z, sizeof(int)));
+  }
+  return e;
+}
+
 // Group-per-row SpMV for the denser coarse operators: G lanes stride a row
 // (coalesced within the group) and combine with a fixed shuffle tree.
 template <class T, int G, int MODE, bool DOT>
@@ -273,6 +444,18 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
       BN_LAUNCH((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);
       break;
+    case 5: {  // row tiles staged by bulk copies (persistent blocks)
+      constexpr int smem = staged_smem_bytes<T>();
+      static bool attr = false;
+      if (!attr) {
+        BN_CUDA(cudaFuncSetAttribute(k_spmv_staged<T, MODE, DOT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr = true;
+      }
+      BN_LAUNCH((k_spmv_staged<T, MODE, DOT>), grid, kRows, smem, s, A.ia, A.ja, A.val, x, A.n,
+                b, y, dw, partial, skip, A.tiles);
+      break;
+    }
     case 8:
       BN_LAUNCH((k_spmv_vec<T, 8, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);

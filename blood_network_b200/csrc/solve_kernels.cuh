@@ -28,9 +28,10 @@ constexpr int kLongRow = 1024;    // rows longer than this get a block each
 constexpr int kLongThreads = 256;
 
 // Non-owning CSR view with values of type T, plus the row-length layout the
-// kernels dispatch on: group == 0 selects the row-tile kernel (short rows),
-// otherwise `group` lanes per row; rows longer than kLongRow are listed in
-// lrows and handled by one block each.
+// kernels dispatch on: group 0-3 select the row-tile kernel (256/128/64/32
+// rows per tile), 5 the row tiles staged by bulk copies, 4/8/32 that many
+// lanes per row; rows longer than kLongRow are listed in lrows and handled
+// by one block each.
 template <class T>
 struct DevMat {
   int n = 0, m = 0, nnz = 0;
@@ -68,6 +69,8 @@ template <class T>
 int spmv(int mode, const DevMat<T>& A, const T* x, const T* b, T* y, cudaStream_t s,
          const T* dot_w = nullptr, double* partial = nullptr);
 int spmv_partials(int n, int nlong);
+// 1 if a bounded wait of the staged SpMV ran out since the last call (then cleared)
+int take_stage_error();
 // Rows of one colour class: rows[t] (or r0 + t when rows is null, a
 // contiguous class); its last nlong rows are long rows (one block each).
 template <class T>

@@ -1279,6 +1279,8 @@ int Solver::pcg(const double* d_b, double* d_x, double tol, int maxiter, int pri
   float ms = 0;
   cudaEventElapsedTime(&ms, ev0, ev1);
   stats.solve_seconds = ms * 1e-3;
+  BN_REQUIRE(take_stage_error() == 0, BN_ERR_SPIN,
+             "staged SpMV: a bounded wait for a bulk copy ran out");
   stats.relres = sqrt(h_sc[SC_RR]) / bnorm;
   stats.bnorm_rel = bn_rel;
   if (iter > maxiter) {
@@ -2021,14 +2023,15 @@ int Solver::autotune_t(int what, double* report, int nreport) {
     if (what & 1) {
       struct Op { const CSR* M; const DBuf<float>* v32; RowLayout* lay; bool packed; const T* x;
                   T* y; int id; };
-      Op ops[3] = {{&L.Ap, &L.A32, &L.layA, L.use_pkA && use_packed, u.p, v.p, 0},
+      Op ops[4] = {{&L.Ap, &L.A32, &L.layA, L.use_pkA && use_packed, u.p, v.p, 0},
                    {&L.Rp, &L.R32, &L.layR, L.use_pkR && use_packed, u.p, cu.p, 1},
-                   {&L.Pp, &L.P32, &L.layP, L.use_pkP && use_packed, cu.p, v.p, 2}};
+                   {&L.Pp, &L.P32, &L.layP, L.use_pkP && use_packed, cu.p, v.p, 2},
+                   {&L.AU, &L.AU32, &L.layAU, !L.split, u.p, v.p, 4}};
       for (Op& op : ops) {
         if (op.packed || op.M->n == 0) continue;
         int best = op.lay->group;
         double best_ms = 1e30;
-        for (int g : {0, 1, 2, 3, 4, 8, 32}) {
+        for (int g : {0, 1, 2, 3, 4, 5, 8, 32}) {
           op.lay->group = g;
           DevMat<T> M = mat<T>(*op.M, op.v32, op.lay);
           const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
