@@ -369,12 +369,10 @@ void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {
   const double avg = A.n > 0 ? (double)A.nnz / A.n : 0.0;
   out.group = avg <= 8.0 ? 0 : (avg <= 16.0 ? 4 : (avg <= 48.0 ? 8 : 32));
   // BN_SPMV_GROUP=g pins every operator to one kernel variant (0-3: row
-  // tiles of 256/128/64/32 rows, 4/8/32: lanes per row); the autotuner may
-  // still change it
+  // tiles of 256/128/64/32 rows, 5: staged 256-row tiles, 4/8/32: lanes per
+  // row); the autotuner may still change it
   static const int forced = getenv("BN_SPMV_GROUP") ? atoi(getenv("BN_SPMV_GROUP")) : -1;
-  if (forced == 0 || forced == 1 || forced == 2 || forced == 3 || forced == 4 || forced == 8 ||
-      forced == 32)
-    out.group = forced;
+  if ((forced >= 0 && forced <= 5) || forced == 8 || forced == 32) out.group = forced;
   DBuf<int> cnt(1, s);
   cnt.zero();
   out.lrows.alloc(A.n > 0 ? A.n : 1, s);

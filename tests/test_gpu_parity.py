@@ -320,7 +320,8 @@ def test_bench_kernel_timings(net20k):
 @pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
 def test_autotuner_choices(net20k, precision):
     """amg_solver_autotune keeps, per level operator, the fastest candidate
-    (SpMV row groups 0/4/8/32, GS lanes 1/8/32); the solve still converges
+    (SpMV row tiles 0-3, staged tiles 5, lanes per row 4/8/32; GS lanes
+    1/8/32), for A, R, P and the split residual operator; the solve still converges
     with the same work."""
     s = _solver(net20k.n, net20k.indptr, net20k.indices, net20k.data, precision=precision)
     x0, it0 = s.solve(net20k.rhs, tol=1e-8)
@@ -328,7 +329,10 @@ def test_autotuner_choices(net20k, precision):
     assert rep.shape[0] >= 3
     for lvl, op, choice, ms in rep:
         assert 0 <= lvl < s.num_levels - 1 and ms > 0
-        assert (choice in (0, 1, 2, 3, 4, 8, 32)) if op < 3 else (choice in (1, 8, 32))
+        if op == 3:
+            assert choice in (1, 8, 32)          # Gauss-Seidel lanes per row
+        else:
+            assert choice in (0, 1, 2, 3, 4, 5, 8, 32)  # SpMV forms (5: staged tiles)
     x1, it1 = s.solve(net20k.rhs, tol=1e-8)
     assert abs(it1 - it0) <= 1
     assert relres(net20k.indptr, net20k.indices, net20k.data, x1, net20k.rhs) <= 1e-8
@@ -359,7 +363,7 @@ def test_row_tile_variants():
         "np.save(sys.argv[1], np.stack(out)); np.save(sys.argv[1] + '.its.npy', np.array(its))\n"
         % root)
     res, its = [], []
-    for g in ("0", "1", "2", "3"):
+    for g in ("0", "1", "2", "3", "5"):
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"tiles_{g}_{os.getpid()}.npy")
         subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
                        env=dict(os.environ, BN_SPMV_GROUP=g))
@@ -368,6 +372,10 @@ def test_row_tile_variants():
         os.remove(path)
         os.remove(path + ".its.npy")
     net = make_config("vascular_20k")
+    # the staged tiles (5) are the 256-row tiles (0) with bulk-copied
+    # operands: same products, same sums, same dot partials, same solves
+    assert res[4].tobytes() == res[0].tobytes()
+    assert np.array_equal(its[4], its[0])
     for r, it in zip(res, its):
         assert np.all(np.abs(it - its[0]) <= 1)
         for x, x0 in zip(r, res[0]):
