@@ -166,12 +166,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// MODE: SPMV_Y / SPMV_RES / SPMV_ADD over rows [0, n) (tiles in the
+// visiting order `tiles`), or kStagedGS: one Gauss-Seidel colour class,
+// rows [r0, r0 + n) with x_i = (b_i - sum_{j != i} a_ij x_j) / d_i in place
+// (into out[t] when out is given), the sum formed as the thread-per-row
+// class kernel forms it.
+constexpr int kStagedGS = 3;
 template <class T, int MODE, bool DOT>
 __global__ void __launch_bounds__(kRows)
 k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
-              const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
-              const T* __restrict__ dw, double* __restrict__ partial, int skip_long,
-              const int* __restrict__ tiles) {
+              const T* x, int n, const T* __restrict__ b, T* y, const T* __restrict__ dw,
+              double* __restrict__ partial, int skip_long, const int* __restrict__ tiles,
+              int r0base, T* __restrict__ out) {
+  constexpr bool kGs = (MODE == kStagedGS);
   extern __shared__ __align__(16) unsigned char stage_mem[];
   __shared__ __align__(8) unsigned long long bar[2];
   __shared__ double red[kRows / 32];
@@ -180,12 +187,13 @@ k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
   auto s_ja = [&](int q) { return (int*)(stage_mem + q * JB); };
   auto s_a = [&](int q) { return (T*)(stage_mem + 2 * JB + q * AB); };
   const int ntiles = (n + kRows - 1) / kRows;
-  auto tile_row = [&](int slot) { return (tiles ? tiles[slot] : slot) * kRows; };
+  auto tile_row = [&](int slot) { return r0base + (tiles ? tiles[slot] : slot) * kRows; };
+  const int rend = r0base + n;
   // thread 0: stage the tile at `slot` into buffer q (or just arrive)
   auto issue = [&](int q, int slot) {
-    const int r0 = tile_row(slot);
-    const int r1 = min(r0 + kRows, n);
-    const int e0 = ia[r0], e1 = ia[r1];
+    const int t0 = tile_row(slot);
+    const int t1 = min(t0 + kRows, rend);
+    const int e0 = ia[t0], e1 = ia[t1];
     const int s0 = e0 & ~3, fl = e1 & ~3;
     if (e1 - e0 <= kStageCap && fl > s0) {
       const unsigned nb = (unsigned)(fl - s0);
@@ -209,20 +217,22 @@ k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
   for (int slot = blockIdx.x; slot < ntiles; slot += gridDim.x, q++) {
     const int st = q & 1;
     if (threadIdx.x == 0 && slot + (int)gridDim.x < ntiles) issue(st ^ 1, slot + gridDim.x);
-    const int r0 = tile_row(slot);
-    const int r1 = min(r0 + kRows, n);
-    const int e0 = ia[r0], e1 = ia[r1];
-    const int i = r0 + threadIdx.x;
+    const int t0 = tile_row(slot);
+    const int t1 = min(t0 + kRows, rend);
+    const int e0 = ia[t0], e1 = ia[t1];
+    const int i = t0 + threadIdx.x;
     int k0 = 0, k1 = 0;
-    T hold = T(0), hw = T(0);
-    if (i < r1) {
+    T hold = T(0), hw = T(0), di = T(1);
+    if (i < t1) {
       k0 = ia[i];
       k1 = ia[i + 1];
-      if (MODE == SPMV_RES) hold = b[i];
+      if (MODE == SPMV_RES || kGs) hold = b[i];
       if (MODE == SPMV_ADD) hold = y[i];
+      if (kGs) di = y[i];  // y: the diagonal (1 where a row has none)
       if (DOT) hw = dw[i];
     }
-    const bool mine = i < r1 && !(skip_long && k1 - k0 > kLongRow);
+    const bool mine = i < t1 && (kGs || !(skip_long && k1 - k0 > kLongRow));
+    T sum = T(0);  // Gauss-Seidel: sum over j != i
     mbar_wait(&bar[st], (unsigned)((q >> 1) & 1));
     const int m = e1 - e0;
     if (m <= kStageCap) {
@@ -240,18 +250,34 @@ k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
         sa[k] = dmul(sa[k], x[sj[k]]);
       __syncthreads();
       if (mine) {
-        for (int k = k0 - s0; k < k1 - s0; k++)
-          hold = (MODE == SPMV_RES) ? dsub(hold, sa[k]) : dadd(hold, sa[k]);
+        for (int k = k0 - s0; k < k1 - s0; k++) {
+          if (kGs) {
+            if (sj[k] != i) sum = dadd(sum, sa[k]);
+          } else {
+            hold = (MODE == SPMV_RES) ? dsub(hold, sa[k]) : dadd(hold, sa[k]);
+          }
+        }
       }
     } else if (mine) {
       for (int k = k0; k < k1; k++) {
-        const T p = dmul(a[k], x[ja[k]]);
-        hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
+        const int j = ja[k];
+        const T p = dmul(a[k], x[j]);
+        if (kGs) {
+          if (j != i) sum = dadd(sum, p);
+        } else {
+          hold = (MODE == SPMV_RES) ? dsub(hold, p) : dadd(hold, p);
+        }
       }
     }
     if (mine) {
-      y[i] = hold;
-      if (DOT) dot += (double)hw * (double)hold;
+      if (kGs) {
+        const T xi = dsub(hold, sum) / di;
+        if (out) out[i - r0base] = xi;
+        else const_cast<T*>(x)[i] = xi;
+      } else {
+        y[i] = hold;
+        if (DOT) dot += (double)hw * (double)hold;
+      }
     }
     __syncthreads();  // both buffers' readers are done before the next issue
   }
@@ -451,7 +477,7 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
         attr = true;
       }
       BN_LAUNCH((k_spmv_staged<T, MODE, DOT>), grid, kRows, smem, s, A.ia, A.ja, A.val, x, A.n,
-                b, y, dw, partial, skip, A.tiles);
+                b, y, dw, partial, skip, A.tiles, 0, (T*)nullptr);
       break;
     }
     case 8:
@@ -588,9 +614,31 @@ __global__ void k_scatter(const int* __restrict__ rows, int r0, int nr, const T*
     x[rows ? rows[t] : r0 + t] = v[t];
 }
 
+// Gauss-Seidel class on the staged row tiles (group 0; contiguous classes)
+template <class T>
+static void gs_staged(const DevMat<T>& A, int r0, int nr, const T* b, T* x, T* out,
+                      const T* d, cudaStream_t s) {
+  if (nr <= 0) return;
+  constexpr int smem = staged_smem_bytes<T>();
+  static bool attr = false;
+  if (!attr) {
+    BN_CUDA(cudaFuncSetAttribute(k_spmv_staged<T, kStagedGS, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  BN_LAUNCH((k_spmv_staged<T, kStagedGS, false>), spmv_grid(nr), kRows, smem, s, A.ia, A.ja,
+            A.val, (const T*)x, nr, b, (T*)d, (const T*)nullptr, (double*)nullptr, 0,
+            (const int*)nullptr, r0, out);
+}
+
 template <class T>
 static void gs_launch(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x,
-                      T* out, int group, cudaStream_t s, int nlong = 0) {
+                      T* out, int group, cudaStream_t s, int nlong = 0, const T* d = nullptr) {
+  if (group == 0 && !rows && d) {  // staged tiles (long rows included: one thread walks each)
+    gs_staged<T>(A, r0, nr, b, x, out, d, s);
+    return;
+  }
+  if (group == 0) group = 1;
   const int nshort = nr - nlong;
   int nb = 0;
   if (nshort > 0)
@@ -620,16 +668,16 @@ template void scatter_range<float>(const float*, int, int, float*, cudaStream_t)
 
 template <class T>
 void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, int group,
-              cudaStream_t s, int nlong) {
+              cudaStream_t s, int nlong, const T* d) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, r0, nr, b, x, nullptr, group, s, nlong);
+  gs_launch<T>(A, rows, r0, nr, b, x, nullptr, group, s, nlong, d);
 }
 
 template <class T>
 void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, T* tmp,
-                  int group, cudaStream_t s, int nlong) {
+                  int group, cudaStream_t s, int nlong, const T* d) {
   if (nr == 0) return;
-  gs_launch<T>(A, rows, r0, nr, b, x, tmp, group, s, nlong);
+  gs_launch<T>(A, rows, r0, nr, b, x, tmp, group, s, nlong, d);
   BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, r0, nr, tmp, x);
 }
 
@@ -960,9 +1008,9 @@ void pcg_scalars(double* sc, int flexible, cudaStream_t s) {
   template int spmv<T>(int, const DevMat<T>&, const T*, const T*, T*, cudaStream_t, const T*,  \
                        double*);                                                             \
   template void gs_color<T>(const DevMat<T>&, const int*, int, int, const T*, T*, int,       \
-                            cudaStream_t, int);                                              \
+                            cudaStream_t, int, const T*);                                    \
   template void jacobi_class<T>(const DevMat<T>&, const int*, int, int, const T*, T*, T*, int,\
-                                cudaStream_t, int);                                          \
+                                cudaStream_t, int, const T*);                                \
   template void vpermute<T>(const T*, const int*, int, T*, bool, cudaStream_t);              \
   template void gs_level_block<T>(const DevMat<T>&, const int*, const int*, int, bool,       \
                                   const T*, T*, T*, cudaStream_t);                           \

@@ -73,12 +73,14 @@ int spmv_partials(int n, int nlong);
 int take_stage_error();
 // Rows of one colour class: rows[t] (or r0 + t when rows is null, a
 // contiguous class); its last nlong rows are long rows (one block each).
+// group: lanes per row (1/8/32), or 0 for the staged row tiles, which need
+// a contiguous class and the diagonal d (1 where a row has none).
 template <class T>
 void gs_color(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, int group,
-              cudaStream_t s, int nlong = 0);
+              cudaStream_t s, int nlong = 0, const T* d = nullptr);
 template <class T>
 void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* b, T* x, T* tmp,
-                  int group, cudaStream_t s, int nlong = 0);
+                  int group, cudaStream_t s, int nlong = 0, const T* d = nullptr);
 // x[r0 + t] = v[t], t < nr
 template <class T>
 void scatter_range(const T* v, int r0, int nr, T* x, cudaStream_t s);

@@ -418,6 +418,11 @@ void Solver::color_level(Level& L, int smoother) {
   }
   const double avg = n > 0 ? (double)L.A.nnz / n : 0.0;
   L.gs_group = avg <= 12.0 ? 1 : (avg <= 48.0 ? 8 : 32);
+  // BN_GS_LANES=g pins the Gauss-Seidel kernel (0 staged row tiles, 1/8/32
+  // lanes per row); the autotuner may still change it
+  static const int gs_forced = getenv("BN_GS_LANES") ? atoi(getenv("BN_GS_LANES")) : -1;
+  if (gs_forced == 0 || gs_forced == 1 || gs_forced == 8 || gs_forced == 32)
+    L.gs_group = gs_forced;
 }
 
 // B = rows perm[new] of A with columns renumbered by cinv (null: unchanged)
@@ -827,14 +832,15 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
           }
           break;
         }
+        const T* dgl = f64 ? (const T*)L.dg.p : (const T*)L.dg32.p;
         for (int q = 0; q < nseg; q++) {
           int c = forward ? q : nseg - 1 - q;
           const int r0 = L.cptr[c];  // classes are contiguous in the solve numbering
           const int nr = L.cptr[c + 1] - r0;
           if (L.cjac[c])
-            jacobi_class<T>(A, nullptr, r0, nr, bb, xl, tmp, L.gs_group, s, L.clong[c]);
+            jacobi_class<T>(A, nullptr, r0, nr, bb, xl, tmp, L.gs_group, s, L.clong[c], dgl);
           else
-            gs_color<T>(A, nullptr, r0, nr, bb, xl, L.gs_group, s, L.clong[c]);
+            gs_color<T>(A, nullptr, r0, nr, bb, xl, L.gs_group, s, L.clong[c], dgl);
         }
         break;
       }
@@ -877,10 +883,11 @@ void Solver::backslash(int l, const T* bb, T* xl, bool zero_guess) {
     // reads only earlier classes: in place), then r = b - A x = AU x
     Phase ph("gs forward (split) + residual", s, l);
     DevMat<T> AL = mat<T>(L.AL, &L.AL32, &L.layAL);
+    const T* dgl = f64 ? (const T*)L.dg.p : (const T*)L.dg32.p;
     const int nseg = (int)L.cptr.size() - 1;
     for (int c = 0; c < nseg; c++) {
       const int r0 = L.cptr[c];
-      gs_color<T>(AL, nullptr, r0, L.cptr[c + 1] - r0, bb, xl, L.gs_group, s, L.clong[c]);
+      gs_color<T>(AL, nullptr, r0, L.cptr[c + 1] - r0, bb, xl, L.gs_group, s, L.clong[c], dgl);
     }
     spmv<T>(SPMV_Y, mat<T>(L.AU, &L.AU32, &L.layAU), xl, nullptr, rr, s);
   } else {
@@ -1865,11 +1872,11 @@ BN_API int amg_solver_bench_kernel(void* h, int which, int precision, int reps, 
             if (f32)
               bn::gs_color<float>(S->mat<float>(L.AL, &L.AL32, &L.layAL), nullptr, r0,
                                   L.cptr[c + 1] - r0, S->g32.p, S->u1f.p, L.gs_group, S->s,
-                                  L.clong[c]);
+                                  L.clong[c], L.dg32.p);
             else
               bn::gs_color<double>(S->mat<double>(L.AL, nullptr, &L.layAL), nullptr, r0,
                                    L.cptr[c + 1] - r0, S->b.p, S->u1.p, L.gs_group, S->s,
-                                   L.clong[c]);
+                                   L.clong[c], L.dg.p);
           }
           if (f32)
             bn::spmv<float>(bn::SPMV_Y, S->mat<float>(L.AU, &L.AU32, &L.layAU), S->u1f.p,
@@ -2048,7 +2055,7 @@ int Solver::autotune_t(int what, double* report, int nreport) {
         !(use_packed && L.use_pkA)) {
       int best = L.gs_group;
       double best_ms = 1e30;
-      for (int g : {1, 8, 32}) {
+      for (int g : {0, 1, 8, 32}) {  // 0: staged row tiles
         L.gs_group = g;
         const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
           smooth<T>(l, v.p, u.p, true);

@@ -330,7 +330,7 @@ def test_autotuner_choices(net20k, precision):
     for lvl, op, choice, ms in rep:
         assert 0 <= lvl < s.num_levels - 1 and ms > 0
         if op == 3:
-            assert choice in (1, 8, 32)          # Gauss-Seidel lanes per row
+            assert choice in (0, 1, 8, 32)       # Gauss-Seidel: staged tiles, lanes per row
         else:
             assert choice in (0, 1, 2, 3, 4, 5, 8, 32)  # SpMV forms (5: staged tiles)
     x1, it1 = s.solve(net20k.rhs, tol=1e-8)
@@ -382,3 +382,33 @@ def test_row_tile_variants():
             assert relres(net.indptr, net.indices, net.data, x, net.rhs) <= 1e-8
             # two solutions of residual < 1e-8 differ by up to cond(A) * 1e-8
             assert np.linalg.norm(x - x0) <= 1e-4 * np.linalg.norm(x0)
+
+
+def test_staged_gauss_seidel_equals_thread_per_row():
+    """The Gauss-Seidel classes on the staged row tiles (BN_GS_LANES=0) form
+    every row's sum as the thread-per-row kernel (BN_GS_LANES=1) does: the
+    same preconditioner application bit for bit, in both precisions (the
+    split first sweep included)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from blood_network_b200 import amg\n"
+        "from blood_network_b200.network import make_config\n"
+        "net = make_config('vascular_20k')\n"
+        "out = []\n"
+        "for prec in (amg.PREC_FP64, amg.PREC_MIXED):\n"
+        "    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=prec)\n"
+        "    out.append(s.precond(net.rhs))\n"
+        "    s.close()\n"
+        "np.save(sys.argv[1], np.stack(out))\n" % root)
+    res = []
+    for g in ("1", "0"):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"gs_{g}_{os.getpid()}.npy")
+        subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
+                       env=dict(os.environ, BN_GS_LANES=g))
+        res.append(np.load(path))
+        os.remove(path)
+    assert res[0].tobytes() == res[1].tobytes()
