@@ -337,8 +337,116 @@ k_tri_batch_m(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
   }
 }
 
+// Tiled form of a many-column sweep: the single-vector tile schedule
+// (IChol::Tiles), a warp per row, lane c (and c + 32) holding column c of
+// the row; every value of the output block doubles as its ready flag (all
+// ones = pending), so each lane polls its own column of a dependency in
+// another tile, time-bounded like the single-vector sweep.  Dependencies in
+// the block's own tile were published before a block barrier.
+template <class T>
+__global__ void __launch_bounds__(512, 2)
+k_tri_tiles_m(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+              const T* __restrict__ diag, const int* __restrict__ rows,
+              const unsigned* __restrict__ imask, const int2* __restrict__ tile_steps,
+              const int2* __restrict__ steps, int ntiles, const T* __restrict__ in, T* out,
+              int K, WaitCtl wc) {
+  using W = WordOf<T>;
+  using U = typename W::U;
+  U* o = reinterpret_cast<U*>(out);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool c0 = lane < K, c1 = lane + 32 < K;
+  for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
+    const int2 ts = tile_steps[q];
+    for (int st = ts.x; st < ts.y; st++) {
+      const int2 sp = steps[st];
+      for (int t = sp.x + w; t < sp.y; t += nw) {
+        const int i = rows[t];
+        const int k0 = ia[t], k1 = ia[t + 1];
+        const unsigned im = imask[t];
+        T s0 = c0 ? in[(size_t)i * K + lane] : T(0);
+        T s1 = c1 ? in[(size_t)i * K + lane + 32] : T(0);
+        for (int k = k0; k < k1; k++) {
+          const int j = ja[k];
+          const T v = val[k];
+          const int bit = k - k0;
+          const bool own = bit < 32 && ((im >> bit) & 1u);
+          if (c0) {
+            const U* p = o + (size_t)j * K + lane;
+            U u = own ? __ldca(p) : ld_relaxed(p);
+            u = wait_word(o, (int)((size_t)j * K + lane), u, W::kPending, W::kNaN, wc, i);
+            if constexpr (sizeof(T) == 8) s0 = xsub(s0, xmul(v, word_value(u)));
+            else s0 = xsubf(s0, xmulf(v, word_value(u)));
+          }
+          if (c1) {
+            const U* p = o + (size_t)j * K + lane + 32;
+            U u = own ? __ldca(p) : ld_relaxed(p);
+            u = wait_word(o, (int)((size_t)j * K + lane + 32), u, W::kPending, W::kNaN, wc, i);
+            if constexpr (sizeof(T) == 8) s1 = xsub(s1, xmul(v, word_value(u)));
+            else s1 = xsubf(s1, xmulf(v, word_value(u)));
+          }
+        }
+        const T d = diag[t];
+        if (c0) {
+          U r = value_word(s0 / d);
+          if (r == W::kPending) r = W::kNaN;
+          st_relaxed(o + (size_t)i * K + lane, r);
+        }
+        if (c1) {
+          U r = value_word(s1 / d);
+          if (r == W::kPending) r = W::kNaN;
+          st_relaxed(o + (size_t)i * K + lane + 32, r);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <class T>
+static void sweep_tiles_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
+  const IChol::Tiles& tl = fwd ? ic.tf : ic.tb;
+  const int* ia = fwd ? ic.fia.p : ic.bia.p;
+  const int* ja = fwd ? ic.vfja.p : ic.vbja.p;
+  const int* rows = fwd ? ic.vorder.p : ic.vborder.p;
+  const T* val;
+  const T* diag;
+  if constexpr (sizeof(T) == 8) {
+    val = fwd ? ic.fval.p : ic.bval.p;
+    diag = fwd ? ic.fdiag.p : ic.bdiag.p;
+  } else {
+    val = fwd ? ic.fval32.p : ic.bval32.p;
+    diag = fwd ? ic.fdiag32.p : ic.bdiag32.p;
+  }
+  BN_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(T) * (size_t)ic.n * K, s));
+  int dev = 0, per_sm = 0, sms = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_tiles_m<T>, 512, 0));
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int cap = sms * per_sm;
+  const int grid = tl.ntiles < cap ? tl.ntiles : cap;
+  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): tiled block sweep grid does not fit");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(512);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_tiles_m<T>, ia, ja, val, diag, rows,
+                             (const unsigned*)tl.imask.p, (const int2*)tl.tile_steps.p,
+                             (const int2*)tl.steps.p, tl.ntiles, in, x, K,
+                             ic.wait.ctl(fwd ? WT_IC_FWD : WT_IC_BWD)));
+}
+
 template <class T>
 void sweep_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
+  if (ic.mode == IChol::kSweepTiles && ic.tf.ntiles > 0 && (size_t)ic.n * K < (1ull << 31)) {
+    sweep_tiles_m<T>(ic, fwd, in, x, K, s);
+    return;
+  }
   const int* ia = fwd ? ic.fia.p : ic.bia.p;
   const int* ja = fwd ? ic.vfja.p : ic.vbja.p;
   const int* rows = fwd ? ic.vorder.p : ic.vborder.p;
@@ -656,6 +764,7 @@ int Solver::pcg_block(int Kin, const double* d_Bcm, double* d_Xcm, double tol, i
              flexible ? 1 : 0, relres, tol, iter, nact_d, s);
     BN_LAUNCH(k_blk_update_p, ge, 256, 0, s, P.p, Z.p, S_(BETA), n0, K);
     nact = read_scalar(nact_d, s);
+    ic.check_waits(s);
   }
   spmm<double>(BM_RES, A, X.p, B.p, AP.p, K, s);
   dot(AP.p, AP.p, S_(RR));
