@@ -443,7 +443,8 @@ static void sweep_tiles_m(const IChol& ic, bool fwd, const T* in, T* x, int K, c
 
 template <class T>
 void sweep_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
-  if (ic.mode == IChol::kSweepTiles && ic.tf.ntiles > 0 && (size_t)ic.n * K < (1ull << 31)) {
+  if (ic.tf.ntiles > 0 && (size_t)ic.n * K < (1ull << 31) &&
+      getenv("BN_BLOCK_IC_LEVELS") == nullptr) {
     sweep_tiles_m<T>(ic, fwd, in, x, K, s);
     return;
   }

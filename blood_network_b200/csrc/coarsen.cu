@@ -30,6 +30,7 @@
 // split therefore differs from the sequential greedy's bucket order; the
 // second pass is the reference's (ordered rule above).
 #include "internal.cuh"
+#include "crand.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -357,25 +358,6 @@ static int count_c(const int* cf, int n, cudaStream_t s) {
   return read_scalar(c.p, s);
 }
 
-// rand() values after srand(12345), drawn from a private generator state:
-// glibc's rand() is random() on its default state (the additive feedback
-// generator with a 128-byte table), and srandom_r/random_r on a table of the
-// same size give the same sequence.
-static void hmis_draws(int* out, int n) {
-  alignas(8) char table[128];
-  struct random_data st;
-  memset(&st, 0, sizeof st);
-  memset(table, 0, sizeof table);
-  BN_REQUIRE(initstate_r(12345u, table, sizeof table, &st) == 0, BN_ERR_ARG,
-             "HMIS: random state");
-  BN_REQUIRE(srandom_r(12345u, &st) == 0, BN_ERR_ARG, "HMIS: random state");
-  for (int i = 0; i < n; i++) {
-    int32_t r;
-    random_r(&st, &r);
-    out[i] = (int)r;
-  }
-}
-
 int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
   (void)max_lam;
   const int n = S.n;
@@ -435,11 +417,11 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
       // ties between equal measures: the reference HMIS's weights
       // lambda_i + rand()/RAND_MAX after srand(12345) (rs_classical.c:
       // 542-551), one draw per point in index order.  The sequence comes
-      // from a private copy of the C library's generator (srandom_r /
-      // random_r, the generator behind srand/rand), so the caller's rand()
-      // state is left alone as the reference's first pass leaves it.
+      // from a restatement of the C library's generator (crand.h), so the
+      // caller's rand() state is left alone as the reference's first pass
+      // leaves it.
       h.resize(n);
-      hmis_draws(h.data(), n);
+      crand_sequence(12345u, h.data(), n);
       rnd.alloc(n, s);
       rnd.upload(h.data(), n);
       BN_LAUNCH(k_pmis_weights, g, 256, 0, s, lam.p, rnd.p, n, w.p, cf);

@@ -165,6 +165,7 @@ k_interp_values_warp(const int* __restrict__ aia, const int* __restrict__ aja,
   __shared__ int s_slot[kInterpWarps][32];  // slot in P's row (C) or -1 (F)
   __shared__ int s_cm[kInterpWarps][32];    // C_i columns by slot
   __shared__ double s_buf[kInterpWarps][32];
+  __shared__ double s_af[kInterpWarps][32];  // a_ik of A (not S) for the strong F points
   __shared__ int s_el[kInterpWarps][32], s_sl[kInterpWarps][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
@@ -172,6 +173,7 @@ k_interp_values_warp(const int* __restrict__ aia, const int* __restrict__ aja,
   int* slt = s_slot[w];
   int* cm = s_cm[w];
   double* buf = s_buf[w];
+  double* af = s_af[w];
   int* el = s_el[w];
   int* sl = s_sl[w];
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -212,6 +214,7 @@ k_interp_values_warp(const int* __restrict__ aia, const int* __restrict__ aja,
             if (col[t] == j) { at = t; break; }
           if (at < 0) cls = 1;
           else if (slt[at] >= 0) pval[p0 + slt[at]] = xadd(pval[p0 + slt[at]], a);  // once per slot
+          else af[at] = a;  // strong F point: its a_ik, from A (a value refresh keeps S's old values)
         }
       }
       const unsigned wm = __ballot_sync(0xffffffffu, cls == 1);
@@ -230,7 +233,7 @@ k_interp_values_warp(const int* __restrict__ aia, const int* __restrict__ aja,
     for (int t = 0; t < ns; t++) {
       if (slt[t] >= 0) continue;
       const int kk = col[t];
-      const double a_ik = sval[s0 + t];
+      const double a_ik = af[t];
       const int h = hubidx ? hubidx[kk] : -1;
       int ne = 0;
       if (h >= 0) {

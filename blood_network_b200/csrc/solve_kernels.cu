@@ -533,12 +533,10 @@ __device__ __forceinline__ void gs_rows_short(const int* __restrict__ ia,
     const int i = rows ? rows[t] : r0 + t;
     T sum = T(0), d = T(0);
     bool has_d = false;
-    // matrix entries are read once per sweep: evict-first, so that L2
-    // keeps x for the gathers
 #pragma unroll 4
     for (int k = ia[i] + gl; k < ia[i + 1]; k += G) {
-      const int j = __ldcs(ja + k);
-      const T v = __ldcs(a + k);
+      const int j = ja[k];
+      const T v = a[k];
       if (j == i) { d = v; has_d = true; }
       else sum = dadd(sum, dmul(v, x[j]));
     }
