@@ -412,3 +412,35 @@ def test_staged_gauss_seidel_equals_thread_per_row():
         res.append(np.load(path))
         os.remove(path)
     assert res[0].tobytes() == res[1].tobytes()
+
+
+def test_ic_sweep_forms_agree():
+    """Every form of the IC(0) triangular sweeps (level launches, one
+    cooperative launch, chunked sync-free, tiled, position-aligned sync-free;
+    BN_IC_MODE) computes each row in the reference's operation order, so the
+    preconditioner application is bit-identical across them, in both
+    precisions."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from blood_network_b200 import amg\n"
+        "from blood_network_b200.network import make_config\n"
+        "net = make_config('vascular_20k')\n"
+        "out = []\n"
+        "for prec in (amg.PREC_FP64, amg.PREC_MIXED):\n"
+        "    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=prec)\n"
+        "    out.append(s.precond(net.rhs))\n"
+        "    s.close()\n"
+        "np.save(sys.argv[1], np.stack(out))\n" % root)
+    res = []
+    for mode in ("flags", "levels", "coop", "tiles", "aligned"):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic_{mode}_{os.getpid()}.npy")
+        subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
+                       env=dict(os.environ, BN_IC_MODE=mode))
+        res.append(np.load(path))
+        os.remove(path)
+    for r in res[1:]:
+        assert r.tobytes() == res[0].tobytes()
