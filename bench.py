@@ -473,6 +473,11 @@ def run_profile(args):
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
         print(f"profiled solve: n={net.n} nnz={net.nnz} iterations={it}", flush=True)
+    elif args.profile == "ic":
+        # one IC(0) solve (two sweeps) per launch, FP32, in the form BN_IC_MODE selects
+        ms = s.bench_kernel(3, 1, reps=20)
+        print(f"ic: n={net.n} nnz={net.nnz} mode={os.environ.get('BN_IC_MODE', 'default')} "
+              f"{ms / 2:.3f} ms per sweep", flush=True)
     else:
         which, prec = (0, 0) if args.profile == "spmv" else (1, 1)
         ms = s.bench_kernel(which, prec, reps=2)
@@ -685,12 +690,12 @@ def main():
                          "over 1%% of the segments of a 10M-node network with respect to every "
                          "segment's log-radius (one forward and one adjoint solve), checked "
                          "against a tighter FP64 gradient and central differences on 50 segments")
-    ap.add_argument("--profile", choices=["solve", "spmv", "gs", "block"], default=None,
+    ap.add_argument("--profile", choices=["solve", "spmv", "gs", "block", "ic"], default=None,
                     help="profiling driver: 'solve' runs one warm-up and one NVTX-scoped "
                          "('profiled_solve') mixed solve; 'spmv'/'gs' run the fine-level FP64 "
                          "residual SpMV / FP32 GS sweep three times after setup; 'block' "
                          "runs one warm-up and one NVTX-scoped ('profiled_block') 16-column "
-                         "block solve")
+                         "block solve; 'ic' times the FP32 IC(0) sweeps")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
