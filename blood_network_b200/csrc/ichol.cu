@@ -579,99 +579,6 @@ __global__ void k_tile_mask(const int* __restrict__ ia, const int* __restrict__ 
   }
 }
 
-// Aligned form: as the sync-free form, but chunk j of every level goes to
-// warp j (mod the warp count), so a warp walks one position window of the
-// level-ordered layout through all levels.  Rows of a level are stored in
-// index order, so on a structured part of the graph a row's nearest earlier
-// neighbours sit at about the same position one level earlier -- computed by
-// the same warp, read back through L1; only the far neighbours come from
-// other warps.  The warp prefetches the next chunk's row data while it
-// finishes the current one.  Every dependency is first read through L1; a
-// pending pattern there (stale or real: each value is written once per
-// sweep and L1 starts clean at a launch) falls back to the bounded polling
-// of the sync-free form.  Progress: a warp takes its chunks in level order,
-// so the lowest unfinished level always has its warps working on it.
-template <class T>
-__device__ __forceinline__ bool next_chunk(const int* __restrict__ lptr, int nlevels, int warp,
-                                           int nwarps, int& l, int& j) {
-  // after chunk j of level l: the same level's next chunk, else the next
-  // level wide enough to hold a chunk for this warp
-  int jn = j + nwarps;
-  if (l >= 0 && jn * 32 < lptr[l + 1] - lptr[l]) { j = jn; return true; }
-  for (int ln = l + 1; ln < nlevels; ln++) {
-    if (warp * 32 < lptr[ln + 1] - lptr[ln]) { l = ln; j = warp; return true; }
-  }
-  l = nlevels;
-  return false;
-}
-
-template <class T>
-__global__ void __launch_bounds__(kFlagThreads)
-k_tri_aligned(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
-              const T* __restrict__ diag, const int* __restrict__ rows,
-              const int* __restrict__ lptr, int nlevels, const T* __restrict__ in, T* out,
-              T* clear, WaitCtl wc) {
-  using W = WordOf<T>;
-  using U = typename W::U;
-  U* o = reinterpret_cast<U*>(out);
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  int l = -1, j = 0;
-  if (!next_chunk<T>(lptr, nlevels, warp, nwarps, l, j)) return;
-  // row data of the current chunk (prefetched)
-  RowPre<T> cur;
-  auto load = [&](RowPre<T>& p, int lv, int jc) {
-    const int t = lptr[lv] + jc * 32 + lane;
-    p.t = t < lptr[lv + 1] ? t : -1;
-    if (p.t >= 0) pre_load<T>(p, t, ia, ja, val, diag, rows, in);
-  };
-  load(cur, l, j);
-  while (l < nlevels) {
-    int ln = l, jn = j;
-    const bool more = next_chunk<T>(lptr, nlevels, warp, nwarps, ln, jn);
-    RowPre<T> nxt;
-    nxt.t = -1;
-    if (more) load(nxt, ln, jn);
-    if (cur.t >= 0) {
-      const int i = cur.i;
-      if (clear) reinterpret_cast<U*>(clear)[i] = W::kPending;
-      T s = cur.in_i;
-      int jj[4];
-      U u[4];
-      const int m = cur.k1 - cur.k0 < kPre ? cur.k1 - cur.k0 : kPre;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        jj[q] = q < m ? cur.j[q] : 0;
-        u[q] = q < m ? __ldca(o + jj[q]) : U(0);
-      }
-      wait_group(o, jj, u, m, W::kPending, W::kNaN, wc, i);
-#pragma unroll
-      for (int q = 0; q < kPre; q++) {
-        if (q < m) {
-          if constexpr (sizeof(T) == 8) s = xsub(s, xmul(cur.v[q], word_value(u[q])));
-          else s = xsubf(s, xmulf(cur.v[q], word_value(u[q])));
-        }
-      }
-      for (int k = cur.k0 + kPre; k < cur.k1; k++) {
-        const int c = ja[k];
-        U w = __ldca(o + c);
-        w = wait_word(o, c, w, W::kPending, W::kNaN, wc, i);
-        if constexpr (sizeof(T) == 8) s = xsub(s, xmul(val[k], word_value(w)));
-        else s = xsubf(s, xmulf(val[k], word_value(w)));
-      }
-      U r = value_word(s / cur.d);
-      if (r == W::kPending) r = W::kNaN;
-      st_relaxed(o + i, r);
-    }
-    __syncwarp();
-    if (!more) break;
-    l = ln;
-    j = jn;
-    cur = nxt;
-  }
-}
-
 // ---------------------------------------------------------------- layout
 __global__ void k_fwd_count(const int* __restrict__ lia, const int* __restrict__ lja,
                             const int* __restrict__ order, int n, int* __restrict__ cnt) {
@@ -1176,32 +1083,6 @@ void IChol::build_tiles(bool forward, cudaStream_t s) {
 }
 
 template <class T>
-static void run_tri_aligned(int nlevels, const int* lptr, int blocks_per_sm, const int* ia,
-                            const int* ja, const T* val, const T* diag, const int* rows,
-                            const T* in, T* out, T* clear, WaitCtl wc, cudaStream_t s) {
-  int dev = 0, per_sm = 0, sms = 0;
-  BN_CUDA(cudaGetDevice(&dev));
-  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_aligned<T>, kFlagThreads,
-                                                        0));
-  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  if (blocks_per_sm > 0 && per_sm > blocks_per_sm) per_sm = blocks_per_sm;
-  const int grid = sms * per_sm;
-  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "IC(0): aligned sweep grid does not fit");
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kFlagThreads);
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
-  attr[0].val.cooperative = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  g_launch_count++;
-  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_aligned<T>, ia, ja, val, diag, rows, lptr, nlevels, in,
-                             out, clear, wc));
-}
-
-template <class T>
 void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
   const T* fv;
   const T* fd;
@@ -1211,15 +1092,6 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
     fv = fval.p; fd = fdiag.p; bv = bval.p; bd = bdiag.p;
   } else {
     fv = fval32.p; fd = fdiag32.p; bv = bval32.p; bd = bdiag32.p;
-  }
-  if (mode == kSweepAligned) {
-    if (n == 0) return;
-    BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
-    run_tri_aligned<T>(nlevels, d_lptr.p, blocks_per_sm, fia.p, vfja.p, fv, fd, vorder.p, b, y, x,
-                       wait.ctl(WT_IC_FWD), s);
-    run_tri_aligned<T>(nlevels, d_bptr.p, blocks_per_sm, bia.p, vbja.p, bv, bd, vborder.p, y, x,
-                       nullptr, wait.ctl(WT_IC_BWD), s);
-    return;
   }
   if (mode == kSweepTiles) {
     if (n == 0) return;
@@ -1351,7 +1223,6 @@ int IChol::mode_from_env() {
   if (!strcmp(v, "levels")) return kSweepLevels;
   if (!strcmp(v, "coop")) return kSweepCoop;
   if (!strcmp(v, "tiles")) return kSweepTiles;
-  if (!strcmp(v, "aligned")) return kSweepAligned;
   return kSweepFlags;
 }
 

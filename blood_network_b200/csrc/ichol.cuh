@@ -27,10 +27,9 @@ struct IChol {
   DBuf<int4> d_cfseg, d_cbseg;  // cooperative schedules (narrow = 1024 rows)
   int n_cfseg = 0, n_cbseg = 0;
   // sweep form: level launches, one cooperative launch with a grid barrier
-  // per level, the sync-free form over 32-row chunks, the tiled form or
-  // the position-aligned sync-free form (BN_IC_MODE=levels|coop|flags|tiles|aligned;
-  // default flags)
-  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3, kSweepAligned = 4 };
+  // per level, the sync-free form over 32-row chunks (default) or the tiled
+  // form (BN_IC_MODE=levels|coop|flags|tiles)
+  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3 };
   int mode = mode_from_env();
   int blocks_per_sm = blocks_from_env();  // sync-free grid: blocks per SM (0: occupancy)
   WaitRecord wait;              // sync-free and tiled forms: bounded waits and their record

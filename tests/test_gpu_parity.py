@@ -416,8 +416,8 @@ def test_staged_gauss_seidel_equals_thread_per_row():
 
 def test_ic_sweep_forms_agree():
     """Every form of the IC(0) triangular sweeps (level launches, one
-    cooperative launch, chunked sync-free, tiled, position-aligned sync-free;
-    BN_IC_MODE) computes each row in the reference's operation order, so the
+    cooperative launch, chunked sync-free, tiled; BN_IC_MODE) computes each
+    row in the reference's operation order, so the
     preconditioner application is bit-identical across them, in both
     precisions."""
     import os
@@ -436,7 +436,7 @@ def test_ic_sweep_forms_agree():
         "    s.close()\n"
         "np.save(sys.argv[1], np.stack(out))\n" % root)
     res = []
-    for mode in ("flags", "levels", "coop", "tiles", "aligned"):
+    for mode in ("flags", "levels", "coop", "tiles"):
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic_{mode}_{os.getpid()}.npy")
         subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
                        env=dict(os.environ, BN_IC_MODE=mode))

@@ -5,8 +5,9 @@ dependencies' values; a wait that runs out raises the sweep's abort word so
 that every other waiting row ends at once, and the host reports the wait
 record as AMG_ERR_SPIN.  Here a chain whose first row is left out of the
 schedule makes row 1 wait for a value that nothing publishes (a flag that
-nothing sets); the launch must end in about one limit, report where it gave
-up, and leave the device usable.
+nothing sets), and every later row waits for its predecessor; the launch
+must end in about one limit, report a row that gave up, and leave the
+device usable.
 """
 import ctypes as C
 
@@ -24,7 +25,13 @@ def test_stalled_sweep_gives_up_within_one_limit(n, limit_ms):
     rc = lib.amg_debug_wait_timeout(n, limit_ms, C.byref(ms))
     msg = lib.amg_solver_last_error().decode()
     assert rc == amg.ERR_SPIN, (rc, msg)
-    assert "row 1 waited" in msg and "for row 0" in msg, msg
+    # every row of the chain waits from the start; the record names the one
+    # whose wait ran out first, a row waiting for its predecessor
+    import re
+    m = re.search(r"row (\d+) waited [0-9.]+ ms for row (\d+)", msg)
+    assert m, msg
+    row, dep = int(m.group(1)), int(m.group(2))
+    assert 1 <= row < n and dep == row - 1, msg
     # one limit for the whole launch, not one per waiting row
     assert limit_ms * 0.9 <= ms.value <= limit_ms + 250.0, (ms.value, msg)
 
