@@ -444,8 +444,8 @@ static void sweep_tiles_m(const IChol& ic, bool fwd, const T* in, T* x, int K, c
 template <class T>
 void sweep_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
   // level launches by default; BN_BLOCK_IC_TILES=1 selects the tiled form
-  // (64 columns on the 5M network: 13.3 ms per right-hand side for the
-  // whole block solve with it, 11.1 ms with level launches)
+  // (64 columns on the 5M network, same run: 13.4 ms per right-hand side for
+  // the whole block solve with it, 11.2 ms with level launches)
   static const bool tiles = getenv("BN_BLOCK_IC_TILES") && atoi(getenv("BN_BLOCK_IC_TILES"));
   if (tiles && ic.tf.ntiles > 0 && (size_t)ic.n * K < (1ull << 31)) {
     sweep_tiles_m<T>(ic, fwd, in, x, K, s);
