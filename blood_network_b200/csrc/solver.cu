@@ -37,7 +37,10 @@ __device__ __forceinline__ unsigned color_hash(unsigned x) {
 // of them taken joins the set's overflow class (colour kMaxColors), which the
 // smoother updates Jacobi-style.
 constexpr int kMaxColors = 32;
-constexpr int kCoarseColors = 2;  // 20M network: 10 iterations at caps 1..8; 2 is fastest with margin
+// 20M network: 10 iterations at caps 1..8; cap 1 measured fastest (mixed
+// 97.2 ms against 99.8 at cap 2 and 104.2 at cap 4; FP64 121.6 / 125.0 /
+// 130.5 ms)
+constexpr int kCoarseColors = 1;
 constexpr double kCapAvgRow = 8.0;  // levels with more entries per row than this are capped
 constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
