@@ -64,6 +64,42 @@ extern std::atomic<unsigned long long> g_launch_count;
     BN_CUDA(cudaGetLastError());                                           \
   } while (0)
 
+// Programmatic dependent launch.  A solve-phase kernel starts with
+// BN_PDL_ENTRY(): it waits until the kernel before it in the stream has
+// finished and its writes are visible (griddepcontrol.wait), then lets the
+// next kernel's blocks be scheduled (griddepcontrol.launch_dependents), so
+// that launch and block scheduling of the next kernel overlap this kernel's
+// tail.  BN_LAUNCH_PDL launches with programmatic stream serialization; only
+// kernels that begin with BN_PDL_ENTRY() may be launched that way (a test
+// checks the sources).  BN_PDL=0 turns it off (plain launches; the entry is
+// then a no-op).
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#define BN_PDL_ENTRY() ::bn::pdl_entry()
+bool pdl_enabled();
+#define BN_LAUNCH_PDL(kern_, grid_, block_, smem_, strm_, ...)                         \
+  do {                                                                                  \
+    ::bn::g_launch_count++;                                                             \
+    if (::bn::pdl_enabled()) {                                                          \
+      cudaLaunchConfig_t cfg_ = {};                                                     \
+      cfg_.gridDim = dim3(grid_);                                                       \
+      cfg_.blockDim = dim3(block_);                                                     \
+      cfg_.dynamicSmemBytes = (smem_);                                                  \
+      cfg_.stream = (strm_);                                                            \
+      cudaLaunchAttribute at_[1];                                                       \
+      at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                  \
+      at_[0].val.programmaticStreamSerializationAllowed = 1;                           \
+      cfg_.attrs = at_;                                                                 \
+      cfg_.numAttrs = 1;                                                                \
+      BN_CUDA(cudaLaunchKernelEx(&cfg_, kern_, __VA_ARGS__));                           \
+    } else {                                                                            \
+      kern_<<<(grid_), (block_), (smem_), (strm_)>>>(__VA_ARGS__);                     \
+      BN_CUDA(cudaGetLastError());                                                      \
+    }                                                                                   \
+  } while (0)
+
 constexpr int kSMs = 148;  // B200: 2 dies x 74 SMs
 
 inline int grid_for(long long n, int block, int per_sm = 16) {

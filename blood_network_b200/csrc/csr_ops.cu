@@ -18,6 +18,11 @@ namespace bn {
 
 std::atomic<unsigned long long> g_launch_count{0};
 
+bool pdl_enabled() {
+  static const bool on = getenv("BN_PDL") == nullptr || atoi(getenv("BN_PDL")) != 0;
+  return on;
+}
+
 bool trace_on() {
   static int on = -1;
   if (on < 0) {

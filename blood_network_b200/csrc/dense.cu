@@ -143,6 +143,7 @@ __global__ void k_xtx(const double* __restrict__ X, int n, double* __restrict__ 
 template <class T>
 __global__ void k_dense_apply(const double* __restrict__ Ainv, int n, const T* __restrict__ b,
                               T* __restrict__ x) {
+  BN_PDL_ENTRY();
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
@@ -191,7 +192,7 @@ void DenseCoarse::setup(const CSR& A, cudaStream_t s) {
 template <class T>
 void DenseCoarse::apply(const T* b, T* x, cudaStream_t s) const {
   if (n == 0) return;
-  BN_LAUNCH(k_dense_apply<T>, grid_for((long long)n * 32, 256, 8), 256, 0, s, inv.p, n, b, x);
+  BN_LAUNCH_PDL(k_dense_apply<T>, grid_for((long long)n * 32, 256, 8), 256, 0, s, inv.p, n, b, x);
 }
 template void DenseCoarse::apply<double>(const double*, double*, cudaStream_t) const;
 template void DenseCoarse::apply<float>(const float*, float*, cudaStream_t) const;

@@ -71,6 +71,7 @@ k_packed(const int* __restrict__ ia, const int* __restrict__ ja, const T* __rest
          const T* x, const T* __restrict__ b, T* y, const T* __restrict__ d,
          const int4* __restrict__ blk, int nblk, const int4* __restrict__ seg, int seg_base,
          const int2* __restrict__ lrow, int* cnt, T* part, int r0) {
+  BN_PDL_ENTRY();
   constexpr bool kGs = (OP == PK_GS || OP == PK_JAC);
   constexpr bool kRowB = (OP != PK_Y);  // per-row b_i (or y_i for ADD)
   if ((int)blockIdx.x < nblk) {
@@ -247,7 +248,7 @@ static void launch_packed(const PackedMat<T>& A, int q, const T* x, const T* b, 
   const int b0 = P.rb[q], nb = P.rb[q + 1] - b0;
   const int s0 = P.rs[q], ns = P.rs[q + 1] - s0;
   if (nb + ns == 0) return;
-  BN_LAUNCH((k_packed<T, OP>), nb + ns, kPackThreads, 0, s, A.ia, A.ja, A.val, x, b, y, d,
+  BN_LAUNCH_PDL((k_packed<T, OP>), nb + ns, kPackThreads, 0, s, A.ia, A.ja, A.val, x, b, y, d,
             P.blk.p + b0, nb, P.seg.p + s0, s0, P.lrow.p, P.cnt.p, (T*)P.part.p, r0);
 }
 

@@ -39,6 +39,7 @@ k_spmv(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restri
        const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
        const T* __restrict__ dw, double* __restrict__ partial, int skip_long,
        const int* __restrict__ tiles) {
+  BN_PDL_ENTRY();
   static_assert(ROWS <= kRows && kRows % ROWS == 0, "tile rows must divide kRows");
   constexpr int SUB = kRows / ROWS;
   __shared__ T prod[kTileNnz];
@@ -178,6 +179,7 @@ k_spmv_staged(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
               const T* x, int n, const T* __restrict__ b, T* y, const T* __restrict__ dw,
               double* __restrict__ partial, int skip_long, const int* __restrict__ tiles,
               int r0base, T* __restrict__ out) {
+  BN_PDL_ENTRY();
   constexpr bool kGs = (MODE == kStagedGS);
   extern __shared__ __align__(16) unsigned char stage_mem[];
   __shared__ __align__(8) unsigned long long bar[2];
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(256)
 k_spmv_vec(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
            const T* __restrict__ x, int n, const T* __restrict__ b, T* __restrict__ y,
            const T* __restrict__ dw, double* __restrict__ partial, int skip_long) {
+  BN_PDL_ENTRY();
   __shared__ double red[8];
   const int gl = threadIdx.x & (G - 1);
   unsigned gmask = 0xffffffffu;
@@ -356,6 +359,7 @@ __global__ void __launch_bounds__(kLongThreads)
 k_spmv_long(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
             const T* __restrict__ x, const int* __restrict__ lrows, const T* __restrict__ b,
             T* __restrict__ y, const T* __restrict__ dw, double* __restrict__ partial) {
+  BN_PDL_ENTRY();
   __shared__ T red[kLongThreads / 32];
   const int i = lrows[blockIdx.x];
   T sum = T(0);
@@ -449,23 +453,23 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
   const int skip = A.lrows != nullptr ? 1 : 0;
   switch (A.group) {
     case 0:
-      BN_LAUNCH((k_spmv<T, MODE, DOT>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dw,
+      BN_LAUNCH_PDL((k_spmv<T, MODE, DOT>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y, dw,
                 partial, skip, A.tiles);
       break;
     case 1:
-      BN_LAUNCH((k_spmv<T, MODE, DOT, 128>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv<T, MODE, DOT, 128>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip, A.tiles);
       break;
     case 2:
-      BN_LAUNCH((k_spmv<T, MODE, DOT, 64>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv<T, MODE, DOT, 64>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip, A.tiles);
       break;
     case 3:
-      BN_LAUNCH((k_spmv<T, MODE, DOT, 32>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv<T, MODE, DOT, 32>), grid, kRows, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip, A.tiles);
       break;
     case 4:
-      BN_LAUNCH((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv_vec<T, 4, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);
       break;
     case 5: {  // row tiles staged by bulk copies (persistent blocks)
@@ -476,21 +480,21 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         attr = true;
       }
-      BN_LAUNCH((k_spmv_staged<T, MODE, DOT>), grid, kRows, smem, s, A.ia, A.ja, A.val, x, A.n,
+      BN_LAUNCH_PDL((k_spmv_staged<T, MODE, DOT>), grid, kRows, smem, s, A.ia, A.ja, A.val, x, A.n,
                 b, y, dw, partial, skip, A.tiles, 0, (T*)nullptr);
       break;
     }
     case 8:
-      BN_LAUNCH((k_spmv_vec<T, 8, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv_vec<T, 8, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);
       break;
     default:
-      BN_LAUNCH((k_spmv_vec<T, 32, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
+      BN_LAUNCH_PDL((k_spmv_vec<T, 32, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);
       break;
   }
   if (A.nlong > 0)
-    BN_LAUNCH((k_spmv_long<T, MODE, DOT>), A.nlong, kLongThreads, 0, s, A.ia, A.ja, A.val, x,
+    BN_LAUNCH_PDL((k_spmv_long<T, MODE, DOT>), A.nlong, kLongThreads, 0, s, A.ia, A.ja, A.val, x,
               A.lrows, b, y, dw, DOT ? partial + grid : nullptr);
 }
 
@@ -597,6 +601,7 @@ __global__ void __launch_bounds__(kLongThreads)
 k_gs_class(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
            const int* __restrict__ rows, int r0, int nshort, int nb_short,
            const T* __restrict__ b, T* x, T* __restrict__ out) {
+  BN_PDL_ENTRY();
   if ((int)blockIdx.x < nb_short) {
     gs_rows_short<T, G>(ia, ja, a, rows, r0, nshort, b, x, out, nb_short);
   } else {
@@ -608,6 +613,7 @@ k_gs_class(const int* __restrict__ ia, const int* __restrict__ ja, const T* __re
 template <class T>
 __global__ void k_scatter(const int* __restrict__ rows, int r0, int nr, const T* __restrict__ v,
                           T* __restrict__ x) {
+  BN_PDL_ENTRY();
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x)
     x[rows ? rows[t] : r0 + t] = v[t];
 }
@@ -624,7 +630,7 @@ static void gs_staged(const DevMat<T>& A, int r0, int nr, const T* b, T* x, T* o
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
-  BN_LAUNCH((k_spmv_staged<T, kStagedGS, false>), spmv_grid(nr), kRows, smem, s, A.ia, A.ja,
+  BN_LAUNCH_PDL((k_spmv_staged<T, kStagedGS, false>), spmv_grid(nr), kRows, smem, s, A.ia, A.ja,
             A.val, (const T*)x, nr, b, (T*)d, (const T*)nullptr, (double*)nullptr, 0,
             (const int*)nullptr, r0, out);
 }
@@ -646,20 +652,20 @@ static void gs_launch(const DevMat<T>& A, const int* rows, int r0, int nr, const
   const int grid = nb + nlong;
   if (grid == 0) return;
   if (group >= 32)
-    BN_LAUNCH((k_gs_class<T, 32>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+    BN_LAUNCH_PDL((k_gs_class<T, 32>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
               nb, b, x, out);
   else if (group >= 8)
-    BN_LAUNCH((k_gs_class<T, 8>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+    BN_LAUNCH_PDL((k_gs_class<T, 8>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
               nb, b, x, out);
   else
-    BN_LAUNCH((k_gs_class<T, 1>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
+    BN_LAUNCH_PDL((k_gs_class<T, 1>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
               nb, b, x, out);
 }
 
 template <class T>
 void scatter_range(const T* v, int r0, int nr, T* x, cudaStream_t s) {
   if (nr == 0) return;
-  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, nullptr, r0, nr, v, x);
+  BN_LAUNCH_PDL(k_scatter<T>, grid_for(nr, 256), 256, 0, s, nullptr, r0, nr, v, x);
 }
 template void scatter_range<double>(const double*, int, int, double*, cudaStream_t);
 template void scatter_range<float>(const float*, int, int, float*, cudaStream_t);
@@ -676,7 +682,7 @@ void jacobi_class(const DevMat<T>& A, const int* rows, int r0, int nr, const T* 
                   int group, cudaStream_t s, int nlong, const T* d) {
   if (nr == 0) return;
   gs_launch<T>(A, rows, r0, nr, b, x, tmp, group, s, nlong, d);
-  BN_LAUNCH(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, r0, nr, tmp, x);
+  BN_LAUNCH_PDL(k_scatter<T>, grid_for(nr, 256), 256, 0, s, rows, r0, nr, tmp, x);
 }
 
 // A whole sweep of a small level in one 1024-thread block: classes in
@@ -687,6 +693,7 @@ __global__ void __launch_bounds__(1024)
 k_gs_level_block(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ a,
                  const int* __restrict__ cptr, const int* __restrict__ cjac, int ncls, int forward,
                  const T* __restrict__ b, T* x, T* tmp) {
+  BN_PDL_ENTRY();
   for (int q = 0; q < ncls; q++) {
     const int c = forward ? q : ncls - 1 - q;
     const int r0 = cptr[c], r1 = cptr[c + 1];
@@ -723,7 +730,7 @@ template <class T>
 void gs_level_block(const DevMat<T>& A, const int* cptr, const int* cjac, int ncls, bool forward,
                     const T* b, T* x, T* tmp, cudaStream_t s) {
   if (ncls <= 0) return;
-  BN_LAUNCH(k_gs_level_block<T>, 1, 1024, 0, s, A.ia, A.ja, A.val, cptr, cjac, ncls,
+  BN_LAUNCH_PDL(k_gs_level_block<T>, 1, 1024, 0, s, A.ia, A.ja, A.val, cptr, cjac, ncls,
             forward ? 1 : 0, b, x, tmp);
 }
 
@@ -731,6 +738,7 @@ void gs_level_block(const DevMat<T>& A, const int* cptr, const int* cjac, int nc
 template <class T>
 __global__ void k_permute(const T* __restrict__ in, const int* __restrict__ map, int n,
                           T* __restrict__ out, int scatter) {
+  BN_PDL_ENTRY();
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     if (scatter) out[map[t]] = in[t];
     else out[t] = in[map[t]];
@@ -738,38 +746,41 @@ __global__ void k_permute(const T* __restrict__ in, const int* __restrict__ map,
 }
 template <class T>
 void vpermute(const T* in, const int* map, int n, T* out, bool scatter, cudaStream_t s) {
-  if (n) BN_LAUNCH(k_permute<T>, grid_for(n, 256), 256, 0, s, in, map, n, out, scatter ? 1 : 0);
+  if (n) BN_LAUNCH_PDL(k_permute<T>, grid_for(n, 256), 256, 0, s, in, map, n, out, scatter ? 1 : 0);
 }
 
 // ------------------------------------------------------------ vector ops
 template <class T>
 __global__ void k_zero(T* __restrict__ x, int n) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = T(0);
 }
 template <class T>
 void vzero(T* x, int n, cudaStream_t s) {
-  if (n) BN_LAUNCH(k_zero<T>, grid_for(n, 256), 256, 0, s, x, n);
+  if (n) BN_LAUNCH_PDL(k_zero<T>, grid_for(n, 256), 256, 0, s, x, n);
 }
 
 template <class TO, class TI>
 __global__ void k_convert(const TI* __restrict__ a, int n, TO* __restrict__ b) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     b[i] = (TO)a[i];
 }
 template <class TO, class TI>
 void vconvert(const TI* a, int n, TO* b, cudaStream_t s) {
-  if (n) BN_LAUNCH((k_convert<TO, TI>), grid_for(n, 256), 256, 0, s, a, n, b);
+  if (n) BN_LAUNCH_PDL((k_convert<TO, TI>), grid_for(n, 256), 256, 0, s, a, n, b);
 }
 
 // x = u + v  (x may alias u)
 template <class T>
 __global__ void k_add(const T* __restrict__ u, const T* __restrict__ v, int n, T* x) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = dadd(u[i], v[i]);
 }
 template <class T>
 void vadd(const T* u, const T* v, int n, T* x, cudaStream_t s) {
-  if (n) BN_LAUNCH(k_add<T>, grid_for(n, 256), 256, 0, s, u, v, n, x);
+  if (n) BN_LAUNCH_PDL(k_add<T>, grid_for(n, 256), 256, 0, s, u, v, n, x);
 }
 
 // block partial sums -> one scalar (deterministic order)
@@ -787,6 +798,7 @@ template <class T>
 __global__ void k_dot2(const T* __restrict__ u, const T* __restrict__ v,
                        const T* __restrict__ w, int n, double* __restrict__ p0,
                        double* __restrict__ p1) {
+  BN_PDL_ENTRY();
   __shared__ double red[32];
   double a = 0.0, c = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -807,23 +819,25 @@ __global__ void k_dot2(const T* __restrict__ u, const T* __restrict__ v,
 template <class T>
 void dot_partials(const T* u, const T* v, const T* w, int n, double* p0, double* p1,
                   cudaStream_t s) {
-  BN_LAUNCH(k_dot2<T>, kRedBlocks, 256, 0, s, u, v, w, n, p0, p1);
+  BN_LAUNCH_PDL(k_dot2<T>, kRedBlocks, 256, 0, s, u, v, w, n, p0, p1);
 }
 
 // y += a u ;  p = z + b p   (uuplmv / umuplv of vector_ops.c with a host scalar)
 __global__ void k_axpy(double* __restrict__ y, const double* __restrict__ u, double a, int n) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = y[i] + u[i] * a;
 }
 __global__ void k_xpby(double* __restrict__ p, const double* __restrict__ z, double b, int n) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     p[i] = z[i] + p[i] * b;
 }
 void vaxpy(double* y, const double* u, double a, int n, cudaStream_t s) {
-  if (n > 0) BN_LAUNCH(k_axpy, grid_for(n, 256), 256, 0, s, y, u, a, n);
+  if (n > 0) BN_LAUNCH_PDL(k_axpy, grid_for(n, 256), 256, 0, s, y, u, a, n);
 }
 void vxpby(double* p, const double* z, double b, int n, cudaStream_t s) {
-  if (n > 0) BN_LAUNCH(k_xpby, grid_for(n, 256), 256, 0, s, p, z, b, n);
+  if (n > 0) BN_LAUNCH_PDL(k_xpby, grid_for(n, 256), 256, 0, s, p, z, b, n);
 }
 
 // ---- segmented PCG (independent systems packed block-diagonally)
@@ -833,6 +847,7 @@ __global__ void __launch_bounds__(256)
 k_seg_dot(const double* __restrict__ u, const double* __restrict__ v,
           const int* __restrict__ ptr, const int* __restrict__ idx, int nseg,
           double* __restrict__ out) {
+  BN_PDL_ENTRY();
   __shared__ double red[32];
   for (int k = blockIdx.x; k < nseg; k += gridDim.x) {
     double a = 0.0;
@@ -847,12 +862,13 @@ k_seg_dot(const double* __restrict__ u, const double* __restrict__ v,
 }
 void seg_dot(const double* u, const double* v, const int* ptr, const int* idx, int nseg,
              double* out, cudaStream_t s) {
-  if (nseg > 0) BN_LAUNCH(k_seg_dot, nseg < 4096 ? nseg : 4096, 256, 0, s, u, v, ptr, idx, nseg, out);
+  if (nseg > 0) BN_LAUNCH_PDL(k_seg_dot, nseg < 4096 ? nseg : 4096, 256, 0, s, u, v, ptr, idx, nseg, out);
 }
 
 // segment of every solve-numbered row: perm[t] is its natural row
 __global__ void k_seg_of_rows(const int* __restrict__ perm, int n, const int* __restrict__ ptr,
                               int nseg, int* __restrict__ seg) {
+  BN_PDL_ENTRY();
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const int r = perm[t];
     int lo = 0, hi = nseg - 1;  // last segment starting at or before r
@@ -865,7 +881,7 @@ __global__ void k_seg_of_rows(const int* __restrict__ perm, int n, const int* __
   }
 }
 void seg_of_rows(const int* perm, int n, const int* ptr, int nseg, int* seg, cudaStream_t s) {
-  if (n > 0) BN_LAUNCH(k_seg_of_rows, grid_for(n, 256), 256, 0, s, perm, n, ptr, nseg, seg);
+  if (n > 0) BN_LAUNCH_PDL(k_seg_of_rows, grid_for(n, 256), 256, 0, s, perm, n, ptr, nseg, seg);
 }
 
 // x += alpha_k p ; r -= alpha_k Ap  (k the row's segment)
@@ -873,6 +889,7 @@ __global__ void k_seg_update_xr(double* __restrict__ x, double* __restrict__ r,
                                 const double* __restrict__ p, const double* __restrict__ ap,
                                 const int* __restrict__ seg, const double* __restrict__ alpha,
                                 int n) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double a = alpha[seg[i]];
     x[i] = x[i] + p[i] * a;
@@ -881,30 +898,32 @@ __global__ void k_seg_update_xr(double* __restrict__ x, double* __restrict__ r,
 }
 void seg_update_xr(double* x, double* r, const double* p, const double* ap, const int* seg,
                    const double* alpha, int n, cudaStream_t s) {
-  if (n > 0) BN_LAUNCH(k_seg_update_xr, grid_for(n, 256), 256, 0, s, x, r, p, ap, seg, alpha, n);
+  if (n > 0) BN_LAUNCH_PDL(k_seg_update_xr, grid_for(n, 256), 256, 0, s, x, r, p, ap, seg, alpha, n);
 }
 
 // p = z + beta_k p
 __global__ void k_seg_update_p(double* __restrict__ p, const double* __restrict__ z,
                                const int* __restrict__ seg, const double* __restrict__ beta,
                                int n) {
+  BN_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     p[i] = z[i] + p[i] * beta[seg[i]];
 }
 void seg_update_p(double* p, const double* z, const int* seg, const double* beta, int n,
                   cudaStream_t s) {
-  if (n > 0) BN_LAUNCH(k_seg_update_p, grid_for(n, 256), 256, 0, s, p, z, seg, beta, n);
+  if (n > 0) BN_LAUNCH_PDL(k_seg_update_p, grid_for(n, 256), 256, 0, s, p, z, seg, beta, n);
 }
 
 // per-segment scalars.  sc layout: [SEG_* * nseg + k]
 __global__ void k_seg_alpha(const double* __restrict__ rz, const double* __restrict__ pap,
                             const int* __restrict__ active, int nseg, double* __restrict__ alpha) {
+  BN_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x)
     alpha[k] = active[k] ? rz[k] / pap[k] : 0.0;
 }
 void seg_alpha(const double* rz, const double* pap, const int* active, int nseg, double* alpha,
                cudaStream_t s) {
-  if (nseg > 0) BN_LAUNCH(k_seg_alpha, grid_for(nseg, 256), 256, 0, s, rz, pap, active, nseg, alpha);
+  if (nseg > 0) BN_LAUNCH_PDL(k_seg_alpha, grid_for(nseg, 256), 256, 0, s, rz, pap, active, nseg, alpha);
 }
 
 // beta (standard or flexible), convergence test, rotate rz; counts the
@@ -916,6 +935,7 @@ __global__ void k_seg_next(double* __restrict__ rz, const double* __restrict__ r
                            double* __restrict__ beta, int nseg, int flexible, int relres,
                            double tol, int iter, const int* __restrict__ iters_done,
                            int* nactive) {
+  BN_PDL_ENTRY();
   if (iters_done) iter = *iters_done + 1;  // device-driven loop: iterations done so far
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nseg; k += gridDim.x * blockDim.x) {
     if (!active[k]) { beta[k] = 0.0; continue; }
@@ -936,12 +956,13 @@ void seg_next(double* rz, const double* rznew, const double* rzold_new, const do
               int nseg, int flexible, int relres, double tol, int iter, int* nactive,
               cudaStream_t s, const int* iters_done) {
   if (nseg > 0)
-    BN_LAUNCH(k_seg_next, grid_for(nseg, 256), 256, 0, s, rz, rznew, rzold_new, rr, bb, rz0,
+    BN_LAUNCH_PDL(k_seg_next, grid_for(nseg, 256), 256, 0, s, rz, rznew, rzold_new, rr, bb, rz0,
               active, iters, beta, nseg, flexible, relres, tol, iter, iters_done, nactive);
 }
 
 // Reduce a partial array into slot `dst` of the scalar block.
 __global__ void k_reduce(const double* __restrict__ part, int m, double* __restrict__ out) {
+  BN_PDL_ENTRY();
   __shared__ double red[32];
   double v = 0.0;
   for (int i = threadIdx.x; i < m; i += blockDim.x) v += part[i];
@@ -949,13 +970,14 @@ __global__ void k_reduce(const double* __restrict__ part, int m, double* __restr
   if (threadIdx.x == 0) *out = t;
 }
 void reduce_partials(const double* part, int m, double* out, cudaStream_t s) {
-  BN_LAUNCH(k_reduce, 1, 1024, 0, s, part, m, out);
+  BN_LAUNCH_PDL(k_reduce, 1, 1024, 0, s, part, m, out);
 }
 
 // x += alpha p ; r -= alpha Ap ; partial r.r     (alpha = sc[RZ] / sc[PAP])
 __global__ void k_pcg_update_xr(double* __restrict__ x, double* __restrict__ r,
                                 const double* __restrict__ p, const double* __restrict__ ap,
                                 int n, const double* __restrict__ sc, double* __restrict__ part) {
+  BN_PDL_ENTRY();
   __shared__ double red[32];
   const double alpha = sc[SC_RZ] / sc[SC_PAP];
   double rr = 0.0;
@@ -970,23 +992,25 @@ __global__ void k_pcg_update_xr(double* __restrict__ x, double* __restrict__ r,
 }
 void pcg_update_xr(double* x, double* r, const double* p, const double* ap, int n,
                    const double* sc, double* part, cudaStream_t s) {
-  BN_LAUNCH(k_pcg_update_xr, kRedBlocks, 256, 0, s, x, r, p, ap, n, sc, part);
+  BN_LAUNCH_PDL(k_pcg_update_xr, kRedBlocks, 256, 0, s, x, r, p, ap, n, sc, part);
 }
 
 // p = z + beta p ; beta from the scalar block (standard or flexible)
 __global__ void k_pcg_update_p(double* __restrict__ p, const double* __restrict__ z, int n,
                                const double* __restrict__ sc) {
+  BN_PDL_ENTRY();
   const double beta = sc[SC_BETA];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     p[i] = beta * p[i] + z[i];         // umuplv: smult * u + v
 }
 void pcg_update_p(double* p, const double* z, int n, const double* sc, cudaStream_t s) {
-  BN_LAUNCH(k_pcg_update_p, grid_for(n, 256), 256, 0, s, p, z, n, sc);
+  BN_LAUNCH_PDL(k_pcg_update_p, grid_for(n, 256), 256, 0, s, p, z, n, sc);
 }
 
 // After z = M r: reduce r.z (and r.z_old), form beta, rotate rz, publish the
 // convergence scalars.  One thread.
 __global__ void k_pcg_scalars(double* sc, int flexible) {
+  BN_PDL_ENTRY();
   const double rz_new = sc[SC_RZNEW];
   double beta;
   if (flexible)
@@ -998,7 +1022,7 @@ __global__ void k_pcg_scalars(double* sc, int flexible) {
   sc[SC_RZ] = rz_new;
 }
 void pcg_scalars(double* sc, int flexible, cudaStream_t s) {
-  BN_LAUNCH(k_pcg_scalars, 1, 1, 0, s, sc, flexible);
+  BN_LAUNCH_PDL(k_pcg_scalars, 1, 1, 0, s, sc, flexible);
 }
 
 // explicit instantiations
