@@ -487,7 +487,7 @@ def run_profile(args):
 
 
 # --------------------------------------------------------------- B200 arm
-def run_adjoint(args, n_nodes=10_000_000, depth=21):
+def run_adjoint(args, n_nodes=10_000_000, depth=21, emit=True, fd=True):
     """Adjoint workload (1 GPU): L = sum over a random 1% of segments of
     (q_e - qhat_e)^2, qhat the flows at log-normally perturbed radii
     (sigma 0.1); dL/d log r for every segment from one forward and one
@@ -537,6 +537,8 @@ def run_adjoint(args, n_nodes=10_000_000, depth=21):
     gp = ref.cpu().numpy()[pick]
     scale = float(torch.abs(ref).max())
     try:
+        if not fd:
+            raise RuntimeError("central differences run in the --adjoint mode only")
         fd = []
         with torch.no_grad():
             for k in pick:
@@ -553,7 +555,9 @@ def run_adjoint(args, n_nodes=10_000_000, depth=21):
                     "median_rel_err": float(np.median(np.abs(fd - gp) /
                                                       np.maximum(np.abs(gp), 1e-300)))}
     except Exception as e:  # a perturbed solve that does not reach 1e-13
-        fd_check = {"segments": 50, "h": h, "error": str(e)}
+        fd_check = ({"segments": 50, "h": h, "error": str(e)} if fd else
+                    {"skipped": "central differences (100 loss evaluations) run in the "
+                                "--adjoint mode only"})
     out = {"metric": "adjoint gradient dL/dlog r, 10M-node network, 1 B200", "impl": "b200",
            "n_gpus": 1, "data": "synthetic", "unit": "s",
            "value": statistics.mean(times),
@@ -566,11 +570,13 @@ def run_adjoint(args, n_nodes=10_000_000, depth=21):
                                   "AMG-PCG, edge kernel, chain to log-radius"},
            "gradient_rel_err_vs_fp64_tol1e-13": rel_ref,
            "fd_check": fd_check}
-    print(json.dumps(out), flush=True)
-    return 0
+    if emit:
+        print(json.dumps(out), flush=True)
+        return 0
+    return out
 
 
-def run_batched(args):
+def run_batched(args, emit=True):
     """Batched workloads: (a) 64 boundary-pressure scenarios of the 5M network
     as one block PCG (per-column scalars, SpMM V-cycle), against the same
     columns solved one at a time on the same hierarchy; (b) 256 networks of
@@ -664,6 +670,8 @@ def run_batched(args):
                      "separate_s_per_network": (sep_setup + sep_solve) / len(nets),
                      "speedup": (sep_setup + sep_solve) / total})
     out["networks_segmented"] = item
+    if not emit:
+        return out
     if rank == 0:
         print(json.dumps(out), flush=True)
     if ws > 1:
@@ -680,6 +688,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and adjoint workloads that the N = 1 headline run "
+                         "also measures (after its timed region)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--batched", action="store_true",
                     help="batched workloads instead of the headline: 64 boundary scenarios on "
@@ -896,6 +907,21 @@ def main():
     del x_tight
 
     lib.amg_solver_free(h)
+    # the batched and adjoint workloads, measured in the same run (N = 1)
+    extras = {}
+    if ws == 1 and not args.no_extras:
+        del d_ia, d_ja, d_val
+        torch.cuda.empty_cache()
+        short = argparse.Namespace(**vars(args))
+        short.steps, short.warmup = min(args.steps, 2), 1
+        try:
+            extras["batched"] = run_batched(short, emit=False)
+        except Exception as e:  # reported, never fatal to the headline line
+            extras["batched"] = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            extras["adjoint"] = run_adjoint(short, emit=False, fd=False)
+        except Exception as e:
+            extras["adjoint"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": mixed_s, "unit": "s", "n_gpus": ws,
@@ -949,6 +975,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist
