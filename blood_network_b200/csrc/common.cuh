@@ -71,8 +71,8 @@ extern std::atomic<unsigned long long> g_launch_count;
 // that launch and block scheduling of the next kernel overlap this kernel's
 // tail.  BN_LAUNCH_PDL launches with programmatic stream serialization; only
 // kernels that begin with BN_PDL_ENTRY() may be launched that way (a test
-// checks the sources).  BN_PDL=0 turns it off (plain launches; the entry is
-// then a no-op).
+// checks the sources).  Off unless BN_PDL=1 (measured slower on the 20M
+// solve); with plain launches the entry is a no-op.
 __device__ __forceinline__ void pdl_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
