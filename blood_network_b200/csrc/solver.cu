@@ -629,10 +629,18 @@ void Solver::build_solve_layout() {
       L.split = false;
       L.AL = CSR();
       L.AU = CSR();
-      if (coloured_level(l) && !(use_packed && L.use_pkA) && L.A.n > kSmallLevel &&
-          L.layA.nlong == 0) {
+      if (coloured_level(l) && L.A.n > kSmallLevel &&
+          ((use_packed && L.use_pkA) || L.layA.nlong == 0)) {
         Phase ph3("split by class", s, l);
         build_split(L);
+        if (use_packed && L.use_pkA) {  // hub rows: the split runs on packed kernels too
+          std::vector<int> hl = host_ia(L.AL, s);
+          std::vector<int2> rg;
+          for (size_t c = 0; c + 1 < L.cptr.size(); c++)
+            rg.push_back(make_int2(L.cptr[c], L.cptr[c + 1]));
+          L.pkAL.build(hl, rg, s);
+          L.pkAU.build(host_ia(L.AU, s), {make_int2(0, L.AU.n)}, s);
+        }
       }
       if (opt.smoother == SMOOTHER_JACOBI || coloured_level(l)) {
         L.dg.alloc(L.A.n, s);
@@ -885,14 +893,21 @@ void Solver::backslash(int l, const T* bb, T* xl, bool zero_guess) {
     // first sweep from x = 0 on AL (every class, Jacobi classes included,
     // reads only earlier classes: in place), then r = b - A x = AU x
     Phase ph("gs forward (split) + residual", s, l);
-    DevMat<T> AL = mat<T>(L.AL, &L.AL32, &L.layAL);
     const T* dgl = f64 ? (const T*)L.dg.p : (const T*)L.dg32.p;
     const int nseg = (int)L.cptr.size() - 1;
-    for (int c = 0; c < nseg; c++) {
-      const int r0 = L.cptr[c];
-      gs_color<T>(AL, nullptr, r0, L.cptr[c + 1] - r0, bb, xl, L.gs_group, s, L.clong[c], dgl);
+    if (use_packed && L.use_pkA) {  // levels with hub rows: packed blocks + row segments
+      PackedMat<T> AL = pmat<T>(L.AL, L.AL32, L.pkAL);
+      for (int c = 0; c < nseg; c++)
+        packed_apply<T>(PK_GS, AL, c, xl, bb, xl, dgl, L.cptr[c], s);
+      packed_apply<T>(PK_Y, pmat<T>(L.AU, L.AU32, L.pkAU), 0, xl, nullptr, rr, nullptr, 0, s);
+    } else {
+      DevMat<T> AL = mat<T>(L.AL, &L.AL32, &L.layAL);
+      for (int c = 0; c < nseg; c++) {
+        const int r0 = L.cptr[c];
+        gs_color<T>(AL, nullptr, r0, L.cptr[c + 1] - r0, bb, xl, L.gs_group, s, L.clong[c], dgl);
+      }
+      spmv<T>(SPMV_Y, mat<T>(L.AU, &L.AU32, &L.layAU), xl, nullptr, rr, s);
     }
-    spmv<T>(SPMV_Y, mat<T>(L.AU, &L.AU32, &L.layAU), xl, nullptr, rr, s);
   } else {
     { Phase ph("gs forward", s, l); smooth<T>(l, bb, xl, true); }
     Phase ph("residual", s, l);
@@ -2036,7 +2051,8 @@ int Solver::autotune_t(int what, double* report, int nreport) {
       Op ops[4] = {{&L.Ap, &L.A32, &L.layA, L.use_pkA && use_packed, u.p, v.p, 0},
                    {&L.Rp, &L.R32, &L.layR, L.use_pkR && use_packed, u.p, cu.p, 1},
                    {&L.Pp, &L.P32, &L.layP, L.use_pkP && use_packed, cu.p, v.p, 2},
-                   {&L.AU, &L.AU32, &L.layAU, !L.split, u.p, v.p, 4}};
+                   {&L.AU, &L.AU32, &L.layAU, !L.split || (use_packed && L.use_pkA), u.p,
+                    v.p, 4}};
       for (Op& op : ops) {
         if (op.packed || op.M->n == 0) continue;
         int best = op.lay->group;

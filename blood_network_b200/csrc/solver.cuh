@@ -58,6 +58,7 @@ struct Level {
   CSR AL, AU;
   DBuf<float> AL32, AU32;
   RowLayout layAL, layAU;
+  Packing pkAL, pkAU;  // levels with hub rows: AL per class, AU as one range
   // work vectors
   DBuf<double> b, x, r;
   DBuf<float> b32, x32, r32;
