@@ -46,6 +46,9 @@ constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
 constexpr int kColorHuge = 4096;    // ... and longer than this by a block
 constexpr int kSmallLevel = 2048;  // levels up to this size (without hub rows) sweep in one block
+// ... and so do levels with at most this many entries, hub rows or not (one
+// block sweeps them faster than one launch per class)
+constexpr long long kSmallLevelNnz = 65536;
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
                               const int* __restrict__ set, int n, const int* __restrict__ color,
@@ -629,7 +632,7 @@ void Solver::build_solve_layout() {
       L.split = false;
       L.AL = CSR();
       L.AU = CSR();
-      if (coloured_level(l) && L.A.n > kSmallLevel &&
+      if (coloured_level(l) && L.A.n > kSmallLevel && L.A.nnz > kSmallLevelNnz &&
           ((use_packed && L.use_pkA) || L.layA.nlong == 0)) {
         Phase ph3("split by class", s, l);
         build_split(L);
@@ -823,7 +826,7 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
         T* tmp = f64 ? (T*)L.r.p : (T*)L.r32.p;
         // small levels sweep in one block, unless they hold hub rows (a warp
         // per row would serialise a class behind them)
-        if (n <= kSmallLevel && L.layA.nlong == 0) {
+        if ((n <= kSmallLevel && L.layA.nlong == 0) || L.A.nnz <= kSmallLevelNnz) {
           gs_level_block<T>(A, L.d_cptr.p, L.d_cjac.p, nseg, forward, bb, xl, tmp, s);
           break;
         }
@@ -2069,7 +2072,7 @@ int Solver::autotune_t(int what, double* report, int nreport) {
         note(l, op.id, best, best_ms);
       }
     }
-    if ((what & 2) && L.cptr.size() > 1 && n > kSmallLevel &&
+    if ((what & 2) && L.cptr.size() > 1 && n > kSmallLevel && L.A.nnz > kSmallLevelNnz &&
         (opt.smoother == SMOOTHER_CF_GS || opt.smoother == SMOOTHER_GS) &&
         !(use_packed && L.use_pkA)) {
       int best = L.gs_group;
