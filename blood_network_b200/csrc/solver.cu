@@ -46,8 +46,7 @@ constexpr int kCappedRounds = 8;    // colouring rounds on capped levels
 constexpr int kColorLong = 256;     // rows longer than this are coloured by a warp
 constexpr int kColorHuge = 4096;    // ... and longer than this by a block
 constexpr int kSmallLevel = 2048;  // levels up to this size (without hub rows) sweep in one block
-// ... and so do levels with at most this many entries, hub rows or not (one
-// block sweeps them faster than one launch per class)
+// levels with at most this many entries take no split first sweep
 constexpr long long kSmallLevelNnz = 65536;
 
 __global__ void k_color_round(const int* __restrict__ ia, const int* __restrict__ ja,
@@ -826,7 +825,7 @@ void Solver::smooth(int l, const T* bb, T* xl, bool forward) {
         T* tmp = f64 ? (T*)L.r.p : (T*)L.r32.p;
         // small levels sweep in one block, unless they hold hub rows (a warp
         // per row would serialise a class behind them)
-        if ((n <= kSmallLevel && L.layA.nlong == 0) || L.A.nnz <= kSmallLevelNnz) {
+        if (n <= kSmallLevel && L.layA.nlong == 0) {
           gs_level_block<T>(A, L.d_cptr.p, L.d_cjac.p, nseg, forward, bb, xl, tmp, s);
           break;
         }
