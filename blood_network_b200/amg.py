@@ -46,7 +46,7 @@ class Stats(C.Structure):
                 ("bnorm_rel", C.c_double), ("setup_seconds", C.c_double),
                 ("solve_seconds", C.c_double), ("num_levels", C.c_int),
                 ("nnz_total", C.c_longlong), ("ichol_levels", C.c_int),
-                ("device_loop", C.c_int)]
+                ("device_loop", C.c_int), ("ichol_form", C.c_int)]
 
 
 class DcsrMat(C.Structure):

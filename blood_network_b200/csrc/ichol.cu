@@ -865,6 +865,11 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   // many-column sweeps of the block PCG
   build_tiles(true, s);
   build_tiles(false, s);
+  if (mode == kSweepSlab) {
+    build_slab_partition(s);
+    build_slab(true, s);
+    build_slab(false, s);
+  }
   ph_lay.done();
   {
     Phase ph("ichol values", s);
@@ -880,6 +885,10 @@ void IChol::remap(const int* inv, cudaStream_t s) {
   vborder.alloc(n, s);
   vfja.alloc(m, s);
   vbja.alloc(m, s);
+  if (mode == kSweepSlab) {
+    slab_pack(sf, inv, s);
+    slab_pack(sb, inv, s);
+  }
   BN_LAUNCH(k_map_ids, grid_for(n, 256), 256, 0, s, order.p, n, inv, vorder.p);
   BN_LAUNCH(k_map_ids, grid_for(n, 256), 256, 0, s, border.p, n, inv, vborder.p);
   if (offd_nnz > 0) {
@@ -917,6 +926,10 @@ void IChol::refresh_values() {
     }
     BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, order.p, n, dpos.p, L.val.p, fdiag32.p);
     BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, border.p, n, dpos.p, L.val.p, bdiag32.p);
+  }
+  if (mode == kSweepSlab) {
+    slab_values(sf, s);
+    slab_values(sb, s);
   }
 }
 
@@ -1100,7 +1113,14 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
     run_tri_tiles<T>(tb, bia.p, vbja.p, bv, bd, vborder.p, y, x, nullptr, wait.ctl(WT_IC_BWD), s);
     return;
   }
-  if (mode == kSweepFlags) {
+  if (slab_ready<T>()) {
+    if (n == 0) return;
+    BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
+    run_tri_slab<T>(*this, true, b, y, x, wait.ctl(WT_IC_FWD), s);
+    run_tri_slab<T>(*this, false, y, x, nullptr, wait.ctl(WT_IC_BWD), s);
+    return;
+  }
+  if (mode == kSweepFlags || mode == kSweepSlab) {
     if (n == 0) return;
     BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
     run_tri_flags<T>(n_fchunk, d_fchunk.p, blocks_per_sm, fia.p, vfja.p, fv, fd, vorder.p, b, y,
@@ -1215,14 +1235,15 @@ void wait_selftest(int n, double limit_ms, double* elapsed_ms, cudaStream_t s) {
 
 int IChol::mode_from_env() {
   // the chunked sync-free form measured fastest for the single-vector sweep
-  // (20M network, FP32: 1.23 ms per sweep against 2.77 ms for the tiled
-  // form, whose block barriers make every level of a tile wait for the
-  // slowest cross-tile dependency)
+  // (20M network, FP32: 1.44 ms per sweep against 1.50 ms for the slab form
+  // and 2.77 ms for the tiled form, whose block barriers make every level of
+  // a tile wait for the slowest cross-tile dependency)
   const char* v = getenv("BN_IC_MODE");
   if (!v) return kSweepFlags;
   if (!strcmp(v, "levels")) return kSweepLevels;
   if (!strcmp(v, "coop")) return kSweepCoop;
   if (!strcmp(v, "tiles")) return kSweepTiles;
+  if (!strcmp(v, "slab")) return kSweepSlab;
   return kSweepFlags;
 }
 

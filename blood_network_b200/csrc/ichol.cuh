@@ -6,6 +6,13 @@
 namespace bn {
 
 __global__ void k_iota_i(int* a, int n);
+// lev[t] = level of position t of a level-ordered layout (ptr: level offsets)
+__global__ void k_pos_level(const int* __restrict__ ptr, int nlevels, int n, int* __restrict__ lev);
+struct IChol;
+// one sweep of the slab form (ic_slab.cu); out pre-filled with the pending pattern
+template <class T>
+void run_tri_slab(const IChol& ic, bool forward, const T* in, T* out, T* clear, WaitCtl wc,
+                  cudaStream_t s);
 
 struct IChol {
   struct Seg {
@@ -27,9 +34,11 @@ struct IChol {
   DBuf<int4> d_cfseg, d_cbseg;  // cooperative schedules (narrow = 1024 rows)
   int n_cfseg = 0, n_cbseg = 0;
   // sweep form: level launches, one cooperative launch with a grid barrier
-  // per level, the sync-free form over 32-row chunks (default) or the tiled
-  // form (BN_IC_MODE=levels|coop|flags|tiles)
-  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3 };
+  // per level, the sync-free form over 32-row chunks (default), the tiled
+  // form or the slab form (the sync-free form runs where its rings do not
+  // fit) (BN_IC_MODE=levels|coop|flags|tiles|slab)
+  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3, kSweepSlab = 4 };
+  static constexpr int kSlabThreads = 512;
   int mode = mode_from_env();
   int blocks_per_sm = blocks_from_env();  // sync-free grid: blocks per SM (0: occupancy)
   WaitRecord wait;              // sync-free and tiled forms: bounded waits and their record
@@ -48,6 +57,40 @@ struct IChol {
     DBuf<unsigned> imask;
   };
   Tiles tf, tb;
+  // slab form: the rows are split into one slab per SM
+  // (rows of wide, index-concentrated levels dealt evenly by their rank in
+  // the level, all other rows by contiguous index ranges); a block owns a
+  // slab and walks its rows in level order, at most kSlabThreads rows per
+  // step with a block barrier after each step.  Row records, entries and
+  // input values are staged into shared-memory rings by asynchronous
+  // copies a few steps ahead; a dependency on a recent row of the same slab
+  // is read from a shared-memory ring of computed values, every other one
+  // from the output vector (value-as-flag, bounded polls), the first of
+  // them pre-read into shared memory when its step is staged.
+  struct Slab {
+    int nsteps = 0, nnz = 0;
+    int lead32 = 0, lead64 = 0;   // staging lead in steps (0: the rings do not fit)
+    DBuf<int2> slab_steps;        // per slab (block): [first step, end step)
+    DBuf<int2> steps;             // nsteps + 1: {first position, first entry}
+    DBuf<int4> rec;               // per position: {vector row, first entry, pre-read dep, FP32 diagonal bits}
+    DBuf<int> rnat, xnat;         // per position: natural row, natural pre-read dep (-1: none)
+    DBuf<int> vrow, vx;           // the same in the vector numbering
+    DBuf<int> cnat, code;         // per entry: ring code (< 0) or dependency (natural / vector numbering)
+    DBuf<int> esrc;               // per entry: index of its value in L
+    DBuf<double> ev64, d64;
+    DBuf<float> ev32, d32;
+  };
+  Slab sf, sb;
+  DBuf<int> slab_of;              // natural row -> slab
+  int nslab = 0;
+  void build_slab_partition(cudaStream_t s);
+  void build_slab(bool forward, cudaStream_t s);
+  void slab_values(Slab& sl, cudaStream_t s);
+  void slab_pack(Slab& sl, const int* inv, cudaStream_t s);
+  template <class T>
+  bool slab_ready() const {
+    return mode == kSweepSlab && (sizeof(T) == 8 ? (sf.lead64 && sb.lead64) : (sf.lead32 && sb.lead32));
+  }
   DBuf<int> fia, fja, fsrc; // forward rows (level order)
   DBuf<int> bia, bja, bsrc; // backward rows (reverse level order)
   // vector indices used by the solves: the rows/columns above mapped into

@@ -212,6 +212,9 @@ typedef struct {
   int device_loop;      /* 1: the last solve ran its PCG iterations as one CUDA
                            graph with the stopping test on the device (no host
                            round trip per iteration); 0: host-driven loop */
+  int ichol_form;       /* form of the fine IC(0) sweeps at the solver's precision:
+                           0 level launches, 1 one cooperative launch, 2 sync-free
+                           32-row chunks, 3 tiles, 4 slabs (one block per SM) */
 } amg_solve_stats;
 
 int amg_solver_stats(void* handle, amg_solve_stats* out);

@@ -436,7 +436,7 @@ def test_ic_sweep_forms_agree():
         "    s.close()\n"
         "np.save(sys.argv[1], np.stack(out))\n" % root)
     res = []
-    for mode in ("flags", "levels", "coop", "tiles"):
+    for mode in ("flags", "levels", "coop", "tiles", "slab"):
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic_{mode}_{os.getpid()}.npy")
         subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
                        env=dict(os.environ, BN_IC_MODE=mode))
@@ -444,3 +444,44 @@ def test_ic_sweep_forms_agree():
         os.remove(path)
     for r in res[1:]:
         assert r.tobytes() == res[0].tobytes()
+
+
+def test_ic_slab_form_on_a_large_network():
+    """On the 2M-node network (a slab per SM holds about one capillary-lattice
+    plane; the tree generations are dealt to the slabs by rank) the slab
+    form is the one that runs when asked for, at both precisions (its
+    staging rings fit), the sync-free form is the default, and the slab
+    form's preconditioner application is bit-identical to the sync-free
+    form's; so are the PCG iterates of a full solve."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from blood_network_b200 import amg\n"
+        "from blood_network_b200.network import make_config\n"
+        "net = make_config('vascular_2m')\n"
+        "out, forms = [], []\n"
+        "for prec in (amg.PREC_FP64, amg.PREC_MIXED):\n"
+        "    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=prec)\n"
+        "    out.append(s.precond(net.rhs))\n"
+        "    out.append(s.solve(net.rhs, tol=1e-8)[0])\n"
+        "    forms.append(s.stats().ichol_form)\n"
+        "    s.close()\n"
+        "np.save(sys.argv[1], np.stack(out))\n"
+        "np.save(sys.argv[1] + '.forms.npy', np.array(forms))\n" % root)
+    res, forms = [], []
+    for mode in (None, "slab"):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic2m_{mode}_{os.getpid()}.npy")
+        env = dict(os.environ)
+        env.pop("BN_IC_MODE", None)
+        if mode:
+            env["BN_IC_MODE"] = mode
+        subprocess.run([sys.executable, "-c", code, path], check=True, timeout=900, env=env)
+        res.append(np.load(path))
+        forms.append(np.load(path + ".forms.npy").tolist())
+        os.remove(path)
+        os.remove(path + ".forms.npy")
+    assert forms == [[2, 2], [4, 4]]
+    assert res[1].tobytes() == res[0].tobytes()
