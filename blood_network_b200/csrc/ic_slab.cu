@@ -52,6 +52,9 @@ namespace {
 constexpr int kNT = IChol::kSlabThreads;
 constexpr int kVS = 1024;  // ring of computed values (positions)
 constexpr int kNS = 64;    // ring of step-table entries
+// chunked slab form: kWT threads per block, 32-row chunks, a tagged ring of
+// kVSW computed values
+constexpr int kWT = 768, kWW = kWT / 32, kVSW = 4096;
 
 template <class T>
 struct SlabRings;
@@ -300,10 +303,11 @@ __global__ void k_slab_runs(const int* __restrict__ perm, const int* __restrict_
   }
 }
 
-// step heads: run starts and every kNT-th position of a run
-__global__ void k_slab_heads(const int* __restrict__ runstart, int n, int* __restrict__ head) {
+// step heads: run starts and every cap-th position of a run
+__global__ void k_slab_heads(const int* __restrict__ runstart, int n, int cap,
+                             int* __restrict__ head) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-    head[p] = ((p - runstart[p]) % kNT) == 0;
+    head[p] = ((p - runstart[p]) % cap) == 0;
 }
 
 __global__ void k_slab_counts(const int* __restrict__ perm, const int* __restrict__ tia,
@@ -337,13 +341,17 @@ __global__ void k_slab_ranges(const int2* __restrict__ steps, const int* __restr
 }
 
 // entries in slab order: ring code for a dependency on the same slab that
-// the ring still holds at the row's step, the natural dependency otherwise
+// the ring still holds when the row is computed, the natural dependency
+// otherwise.  Stepped form: code ~slot, held while the dependency is at most
+// kVS positions before the end of the row's step.  Chunked form: code
+// -(distance back), held while the distance is at most kVSW less the
+// positions a block has in flight (kWW chunks of 32).
 __global__ void k_slab_entries(const int* __restrict__ perm, const int* __restrict__ keys,
                                const int* __restrict__ sid, const int2* __restrict__ steps,
                                const int* __restrict__ eo, const int* __restrict__ tia,
                                const int* __restrict__ tja, const int* __restrict__ tsrc,
                                const int* __restrict__ slab_of, const int* __restrict__ newpos,
-                               int n, int* __restrict__ cnat, int* __restrict__ esrc,
+                               int n, int chunked, int* __restrict__ cnat, int* __restrict__ esrc,
                                int* __restrict__ xnat) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const int t = perm[p], q = keys[p];
@@ -353,8 +361,16 @@ __global__ void k_slab_entries(const int* __restrict__ perm, const int* __restri
     for (int m = 0; m < c; m++) {
       const int j = tja[b + m];
       const int qp = newpos[j];
-      const bool ring = slab_of[j] == q && qp >= p1 - kVS;
-      cnat[o + m] = ring ? ~(qp & (kVS - 1)) : j;
+      bool ring;
+      int code;
+      if (chunked) {
+        ring = slab_of[j] == q && p - qp <= kVSW - 32 * kWW;
+        code = qp - p;
+      } else {
+        ring = slab_of[j] == q && qp >= p1 - kVS;
+        code = ~(qp & (kVS - 1));
+      }
+      cnat[o + m] = ring ? code : j;
       esrc[o + m] = tsrc[b + m];
       if (!ring && xs < 0) xs = j;
     }
@@ -511,6 +527,269 @@ bool slab_fits_device() {
   return per_sm >= 1;
 }
 
+// ------------------------------------------------------------ chunked form
+// The same slabs without block barriers: the warps of a block take the
+// slab's 32-row chunks (cut at level boundaries) in order, chunk c to warp
+// c mod kWW, and a row waits only for its own dependencies: a recent row of
+// the slab through a ring of computed values in shared memory, each slot
+// tagged with the position it holds (a reader waits for its position's
+// tag), every other dependency through the output vector as in the
+// sync-free form.  A warp starts chunk c only when every warp of the block
+// is past chunk c - kWW (progress words in shared memory), so a block has at
+// most kWW chunks in flight and a slot is rewritten (position q + kVSW)
+// only after every reader of q has read it.
+// Each warp loads the records of its chunk after next and the inputs and
+// entries of its next chunk before it works on the current one.
+template <class T>
+struct ChunkRec {
+  int p, p1, e1;  // this lane's position, the chunk's end position and end entry
+  int4 r;         // record (r.y: first entry)
+};
+template <class T>
+struct ChunkDat {
+  T in, d;
+  int cnt;        // entries of the row
+  int code[4];
+  T val[4];
+};
+
+template <class T>
+__device__ __forceinline__ ChunkRec<T> chunk_rec(const SlabArgs<T>& a, int c, int s1, int lane) {
+  ChunkRec<T> q;
+  q.p = 0;
+  q.p1 = 0;
+  q.e1 = 0;
+  q.r = make_int4(0, 0, -1, 0);
+  if (c < s1) {
+    const int2 b0 = a.steps[c], b1 = a.steps[c + 1];
+    q.p = b0.x + lane;
+    q.p1 = b1.x;
+    q.e1 = b1.y;
+    if (q.p < q.p1) q.r = a.rec[q.p];
+  }
+  return q;
+}
+
+template <class T>
+__device__ __forceinline__ ChunkDat<T> chunk_dat(const SlabArgs<T>& a, const ChunkRec<T>& q) {
+  ChunkDat<T> d;
+  const int nxt = __shfl_down_sync(0xffffffffu, q.r.y, 1);
+  d.cnt = 0;
+  d.in = T(0);
+  d.d = T(1);
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    d.code[t] = 0;
+    d.val[t] = T(0);
+  }
+  if (q.p < q.p1) {
+    const int e1 = q.p + 1 < q.p1 ? nxt : q.e1;
+    d.cnt = e1 - q.r.y;
+    d.in = a.in[q.r.x];
+    if constexpr (sizeof(T) == 8) d.d = a.d[q.p];
+    else d.d = __int_as_float(q.r.w);
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+      if (t < d.cnt) {
+        d.code[t] = a.code[q.r.y + t];
+        d.val[t] = a.ev[q.r.y + t];
+      }
+    }
+  }
+  return d;
+}
+
+// Value of position q from the ring (waits for its tag; bounded).
+template <class T>
+__device__ __forceinline__ typename WordOf<T>::U ring_get(unsigned long long* sR, int* sTag,
+                                                          int q, const WaitCtl& wc, int row) {
+  using U = typename WordOf<T>::U;
+  const int slot = q & (kVSW - 1);
+  unsigned long long t0 = 0;
+  for (int it = 0;; it++) {
+    if constexpr (sizeof(T) == 4) {
+      const unsigned long long v = *reinterpret_cast<volatile unsigned long long*>(&sR[slot]);
+      if ((int)(unsigned)(v & 0xffffffffull) == q) return (U)(v >> 32);
+    } else {
+      if (*reinterpret_cast<volatile int*>(&sTag[slot]) == q) {
+        __threadfence_block();
+        return (U)(*reinterpret_cast<volatile unsigned long long*>(&sR[slot]));
+      }
+    }
+    bool ran_out = false;
+    if (it >= kSpinFast && wait_backoff(wc, it, t0, &ran_out)) {
+      if (ran_out) wait_give_up(wc, row, q, global_ns() - t0);
+      return WordOf<T>::kNaN;
+    }
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void ring_put(unsigned long long* sR, int* sTag, int p,
+                                         typename WordOf<T>::U w) {
+  const int slot = p & (kVSW - 1);
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<volatile unsigned long long*>(&sR[slot]) =
+        ((unsigned long long)w << 32) | (unsigned)p;
+  } else {
+    *reinterpret_cast<volatile unsigned long long*>(&sR[slot]) = w;
+    __threadfence_block();
+    *reinterpret_cast<volatile int*>(&sTag[slot]) = p;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWT, 1) k_tri_slabw(SlabArgs<T> a) {
+  using Wd = WordOf<T>;
+  using U = typename Wd::U;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int sProg[kWW];  // per warp: its next chunk (all its earlier ones done)
+  unsigned long long* sR = reinterpret_cast<unsigned long long*>(smem);
+  int* sTag = reinterpret_cast<int*>(sR + kVSW);  // FP64 only
+  U* o = reinterpret_cast<U*>(a.out);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int2 ss = a.slab_steps[blockIdx.x];
+  const int s0 = ss.x, s1 = ss.y;
+  if (s0 >= s1) return;
+  for (int i = tid; i < kVSW; i += kWT) {
+    if constexpr (sizeof(T) == 4) sR[i] = 0xffffffffull;  // tag -1
+    else sTag[i] = -1;
+  }
+  if (tid < kWW) sProg[tid] = s0 + tid;
+  __syncthreads();
+  int c = s0 + w;
+  ChunkRec<T> r0 = chunk_rec(a, c, s1, lane);
+  ChunkRec<T> r1 = chunk_rec(a, c + kWW, s1, lane);
+  ChunkDat<T> d0 = chunk_dat(a, r0);
+  for (; c < s1; c += kWW) {
+    const ChunkRec<T> r2 = chunk_rec(a, c + 2 * kWW, s1, lane);
+    const ChunkDat<T> d1 = chunk_dat(a, r1);
+    {  // gate: no warp of the block more than kWW chunks behind
+      unsigned long long t0 = 0;
+      for (int it = 0;; it++) {
+        int m = lane < kWW ? *reinterpret_cast<volatile int*>(&sProg[lane]) : 0x7fffffff;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const int v = __shfl_xor_sync(0xffffffffu, m, off);
+          m = v < m ? v : m;
+        }
+        if (c < m + kWW) break;
+        bool ran_out = false;
+        if (it >= kSpinFast && wait_backoff(a.wc, it, t0, &ran_out)) {
+          if (ran_out && lane == 0) wait_give_up(a.wc, -1, c, global_ns() - t0);
+          break;
+        }
+      }
+    }
+    if (r0.p < r0.p1) {
+      const int p = r0.p, vi = r0.r.x;
+      T s = d0.in;
+      for (int e = 0; e < d0.cnt; e += 4) {
+        const int m = d0.cnt - e < 4 ? d0.cnt - e : 4;
+        int j[4];
+        T v[4];
+        U u[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          j[t] = 0;
+          v[t] = T(0);
+          u[t] = U(0);
+          if (t < m) {
+            int cd;
+            if (e == 0) {
+              cd = d0.code[t];
+              v[t] = d0.val[t];
+            } else {
+              cd = a.code[r0.r.y + e + t];
+              v[t] = a.ev[r0.r.y + e + t];
+            }
+            if (cd < 0) {
+              u[t] = ring_get<T>(sR, sTag, p + cd, a.wc, vi);
+            } else {
+              j[t] = cd;
+              u[t] = ld_relaxed(o + cd);
+            }
+          }
+        }
+        wait_group(o, j, u, m, Wd::kPending, Wd::kNaN, a.wc, vi);
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          if (t < m) {
+            if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[t], word_value(u[t])));
+            else s = xsubf(s, xmulf(v[t], word_value(u[t])));
+          }
+        }
+      }
+      U res = value_word(s / d0.d);
+      if (res == Wd::kPending) res = Wd::kNaN;
+      ring_put<T>(sR, sTag, p, res);
+      st_relaxed(o + vi, res);
+      if (a.clear) reinterpret_cast<U*>(a.clear)[vi] = Wd::kPending;
+    }
+    __syncwarp();
+    if (lane == 0) *reinterpret_cast<volatile int*>(&sProg[w]) = c + kWW;
+    r0 = r1;
+    r1 = r2;
+    d0 = d1;
+  }
+}
+
+template <class T>
+constexpr size_t slabw_smem_bytes() {
+  return (size_t)kVSW * 8 + (sizeof(T) == 8 ? (size_t)kVSW * 4 : 0);
+}
+
+template <class T>
+bool slab_fits_chunked() {
+  int per_sm = 0;
+  BN_CUDA(cudaFuncSetAttribute(k_tri_slabw<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)slabw_smem_bytes<T>()));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_slabw<T>, kWT,
+                                                        slabw_smem_bytes<T>()));
+  return per_sm >= 1;
+}
+
+template <class T>
+void slabw_launch(const IChol::Slab& sl, int nslab, const T* d, const T* ev, const T* in, T* out,
+                  T* clear, WaitCtl wc, cudaStream_t s) {
+  constexpr size_t smem = slabw_smem_bytes<T>();
+  static std::atomic<unsigned long long> attr_set{0};
+  int dev = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
+    BN_CUDA(cudaFuncSetAttribute(k_tri_slabw<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    attr_set.fetch_or(bit);
+  }
+  SlabArgs<T> a;
+  a.slab_steps = sl.slab_steps.p;
+  a.steps = sl.steps.p;
+  a.rec = sl.rec.p;
+  a.code = sl.code.p;
+  a.ev = ev;
+  a.d = d;
+  a.in = in;
+  a.out = out;
+  a.clear = clear;
+  a.wc = wc;
+  a.preread = 0;
+  a.trace = nullptr;
+  a.trace_cap = 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nslab);
+  cfg.blockDim = dim3(kWT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_slabw<T>, a));
+}
+
 }  // namespace
 
 // One slab per SM.  A level of which a slab of consecutive rows would hold
@@ -589,7 +868,8 @@ void IChol::build_slab(bool forward, cudaStream_t s) {
     DBuf<unsigned char> t(tmp, s);
     BN_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, hv.p, runstart.p, MaxOp(), n, s));
   }
-  BN_LAUNCH(k_slab_heads, g, 256, 0, s, runstart.p, n, head.p);
+  const bool chunked = mode == kSweepSlabW;
+  BN_LAUNCH(k_slab_heads, g, 256, 0, s, runstart.p, n, chunked ? 32 : kNT, head.p);
   tmp = 0;
   BN_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, head.p, sid.p, n, s));
   {
@@ -608,8 +888,12 @@ void IChol::build_slab(bool forward, cudaStream_t s) {
   BN_LAUNCH(k_slab_ranges, grid_for(nsteps, 256), 256, 0, s, sl.steps.p, keys.p, nsteps,
             sl.slab_steps.p);
   BN_LAUNCH(k_slab_entries, g, 256, 0, s, perm.p, keys.p, sid.p, sl.steps.p, eo.p, tia, tja, tsrc,
-            slab_of.p, newpos.p, n, sl.cnat.p, sl.esrc.p, sl.xnat.p);
+            slab_of.p, newpos.p, n, chunked ? 1 : 0, sl.cnat.p, sl.esrc.p, sl.xnat.p);
   BN_LAUNCH(k_slab_init_rec, g, 256, 0, s, eo.p, n, sl.rec.p);
+  if (chunked) {  // no staging rings: the chunked kernel only needs its value ring
+    sl.lead32 = slab_fits_chunked<float>() ? 1 : 0;
+    sl.lead64 = slab_fits_chunked<double>() ? 1 : 0;
+  } else {
   // ring fit for the staging leads
   DBuf<int> w(6, s);
   w.zero();
@@ -640,6 +924,7 @@ void IChol::build_slab(bool forward, cudaStream_t s) {
             "lead 3: %d/%d/%d (records/inputs/entries); lead FP32 %d, FP64 %d\n",
             forward ? "forward" : "backward", nslab, nsteps, hw[0], hw[1], hw[2], hw[3], hw[4],
             hw[5], sl.lead32, sl.lead64);
+  }
   // vector numbering: natural until remap()
   BN_LAUNCH(k_slab_vids, g, 256, 0, s, sl.rnat.p, sl.xnat.p, n, (const int*)nullptr, sl.vrow.p,
             sl.vx.p);
@@ -688,6 +973,13 @@ template <class T>
 void run_tri_slab(const IChol& ic, bool forward, const T* in, T* out, T* clear, WaitCtl wc,
                   cudaStream_t s) {
   const IChol::Slab& sl = forward ? ic.sf : ic.sb;
+  if (ic.mode == IChol::kSweepSlabW) {
+    if constexpr (sizeof(T) == 8)
+      slabw_launch<double>(sl, ic.nslab, sl.d64.p, sl.ev64.p, in, out, clear, wc, s);
+    else
+      slabw_launch<float>(sl, ic.nslab, (const float*)nullptr, sl.ev32.p, in, out, clear, wc, s);
+    return;
+  }
   if constexpr (sizeof(T) == 8) {
     if (sl.lead64 == 3)
       slab_launch<double, 3>(sl, ic.nslab, sl.d64.p, sl.ev64.p, in, out, clear, wc, s);

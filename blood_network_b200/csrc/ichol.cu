@@ -865,7 +865,7 @@ void IChol::finish(const int* aia, const int* aja, const double* aval, bool nume
   // many-column sweeps of the block PCG
   build_tiles(true, s);
   build_tiles(false, s);
-  if (mode == kSweepSlab) {
+  if (mode == kSweepSlab || mode == kSweepSlabW) {
     build_slab_partition(s);
     build_slab(true, s);
     build_slab(false, s);
@@ -885,7 +885,7 @@ void IChol::remap(const int* inv, cudaStream_t s) {
   vborder.alloc(n, s);
   vfja.alloc(m, s);
   vbja.alloc(m, s);
-  if (mode == kSweepSlab) {
+  if (mode == kSweepSlab || mode == kSweepSlabW) {
     slab_pack(sf, inv, s);
     slab_pack(sb, inv, s);
   }
@@ -927,7 +927,7 @@ void IChol::refresh_values() {
     BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, order.p, n, dpos.p, L.val.p, fdiag32.p);
     BN_LAUNCH(k_gather_diag<float>, g, 256, 0, s, border.p, n, dpos.p, L.val.p, bdiag32.p);
   }
-  if (mode == kSweepSlab) {
+  if (mode == kSweepSlab || mode == kSweepSlabW) {
     slab_values(sf, s);
     slab_values(sb, s);
   }
@@ -1120,7 +1120,7 @@ void IChol::solve(const T* b, T* y, T* x, cudaStream_t s) {
     run_tri_slab<T>(*this, false, y, x, nullptr, wait.ctl(WT_IC_BWD), s);
     return;
   }
-  if (mode == kSweepFlags || mode == kSweepSlab) {
+  if (mode == kSweepFlags || mode == kSweepSlab || mode == kSweepSlabW) {
     if (n == 0) return;
     BN_CUDA(cudaMemsetAsync(y, 0xFF, sizeof(T) * (size_t)n, s));
     run_tri_flags<T>(n_fchunk, d_fchunk.p, blocks_per_sm, fia.p, vfja.p, fv, fd, vorder.p, b, y,
@@ -1244,6 +1244,7 @@ int IChol::mode_from_env() {
   if (!strcmp(v, "coop")) return kSweepCoop;
   if (!strcmp(v, "tiles")) return kSweepTiles;
   if (!strcmp(v, "slab")) return kSweepSlab;
+  if (!strcmp(v, "slabw")) return kSweepSlabW;
   return kSweepFlags;
 }
 

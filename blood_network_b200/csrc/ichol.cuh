@@ -36,8 +36,12 @@ struct IChol {
   // sweep form: level launches, one cooperative launch with a grid barrier
   // per level, the sync-free form over 32-row chunks (default), the tiled
   // form or the slab form (the sync-free form runs where its rings do not
-  // fit) (BN_IC_MODE=levels|coop|flags|tiles|slab)
-  enum { kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3, kSweepSlab = 4 };
+  // fit) or its chunked variant without barriers
+  // (BN_IC_MODE=levels|coop|flags|tiles|slab|slabw)
+  enum {
+    kSweepLevels = 0, kSweepCoop = 1, kSweepFlags = 2, kSweepTiles = 3, kSweepSlab = 4,
+    kSweepSlabW = 5
+  };
   static constexpr int kSlabThreads = 512;
   int mode = mode_from_env();
   int blocks_per_sm = blocks_from_env();  // sync-free grid: blocks per SM (0: occupancy)
@@ -89,7 +93,8 @@ struct IChol {
   void slab_pack(Slab& sl, const int* inv, cudaStream_t s);
   template <class T>
   bool slab_ready() const {
-    return mode == kSweepSlab && (sizeof(T) == 8 ? (sf.lead64 && sb.lead64) : (sf.lead32 && sb.lead32));
+    return (mode == kSweepSlab || mode == kSweepSlabW) &&
+           (sizeof(T) == 8 ? (sf.lead64 && sb.lead64) : (sf.lead32 && sb.lead32));
   }
   DBuf<int> fia, fja, fsrc; // forward rows (level order)
   DBuf<int> bia, bja, bsrc; // backward rows (reverse level order)

@@ -1953,7 +1953,8 @@ BN_API int amg_solver_stats(void* h, amg_solve_stats* out) {
     const bool f32 = S->opt.precision == AMG_PREC_MIXED;
     const int m = S->ic.mode;
     const bool slab = f32 ? S->ic.slab_ready<float>() : S->ic.slab_ready<double>();
-    S->stats.ichol_form = m == bn::IChol::kSweepSlab ? (slab ? 4 : 2) : m;
+    S->stats.ichol_form =
+        (m == bn::IChol::kSweepSlab || m == bn::IChol::kSweepSlabW) ? (slab ? m : 2) : m;
   }
   *out = S->stats;
   return 0;

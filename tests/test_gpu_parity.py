@@ -436,7 +436,7 @@ def test_ic_sweep_forms_agree():
         "    s.close()\n"
         "np.save(sys.argv[1], np.stack(out))\n" % root)
     res = []
-    for mode in ("flags", "levels", "coop", "tiles", "slab"):
+    for mode in ("flags", "levels", "coop", "tiles", "slab", "slabw"):
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic_{mode}_{os.getpid()}.npy")
         subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600,
                        env=dict(os.environ, BN_IC_MODE=mode))
@@ -449,10 +449,11 @@ def test_ic_sweep_forms_agree():
 def test_ic_slab_form_on_a_large_network():
     """On the 2M-node network (a slab per SM holds about one capillary-lattice
     plane; the tree generations are dealt to the slabs by rank) the slab
-    form is the one that runs when asked for, at both precisions (its
-    staging rings fit), the sync-free form is the default, and the slab
-    form's preconditioner application is bit-identical to the sync-free
-    form's; so are the PCG iterates of a full solve."""
+    form and its chunked variant are the ones that run when asked for, at
+    both precisions (the staging rings fit), the sync-free form is the
+    default, and both slab forms' preconditioner applications are
+    bit-identical to the sync-free form's; so are the PCG iterates of a full
+    solve."""
     import os
     import subprocess
     import sys
@@ -472,7 +473,7 @@ def test_ic_slab_form_on_a_large_network():
         "np.save(sys.argv[1], np.stack(out))\n"
         "np.save(sys.argv[1] + '.forms.npy', np.array(forms))\n" % root)
     res, forms = [], []
-    for mode in (None, "slab"):
+    for mode in (None, "slab", "slabw"):
         path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"ic2m_{mode}_{os.getpid()}.npy")
         env = dict(os.environ)
         env.pop("BN_IC_MODE", None)
@@ -483,5 +484,6 @@ def test_ic_slab_form_on_a_large_network():
         forms.append(np.load(path + ".forms.npy").tolist())
         os.remove(path)
         os.remove(path + ".forms.npy")
-    assert forms == [[2, 2], [4, 4]]
-    assert res[1].tobytes() == res[0].tobytes()
+    assert forms == [[2, 2], [4, 4], [5, 5]]
+    for r in res[1:]:
+        assert r.tobytes() == res[0].tobytes()
