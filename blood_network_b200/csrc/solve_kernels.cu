@@ -399,10 +399,11 @@ void analyze_rows(const CSR& A, RowLayout& out, cudaStream_t s) {
   const double avg = A.n > 0 ? (double)A.nnz / A.n : 0.0;
   out.group = avg <= 8.0 ? 0 : (avg <= 16.0 ? 4 : (avg <= 48.0 ? 8 : 32));
   // BN_SPMV_GROUP=g pins every operator to one kernel variant (0-3: row
-  // tiles of 256/128/64/32 rows, 5: staged 256-row tiles, 4/8/32: lanes per
-  // row); the autotuner may still change it
+  // tiles of 256/128/64/32 rows, 5: staged 256-row tiles, 4/8/16/32: lanes
+  // per row); the autotuner may still change it
   static const int forced = getenv("BN_SPMV_GROUP") ? atoi(getenv("BN_SPMV_GROUP")) : -1;
-  if ((forced >= 0 && forced <= 5) || forced == 8 || forced == 32) out.group = forced;
+  if ((forced >= 0 && forced <= 5) || forced == 8 || forced == 16 || forced == 32)
+    out.group = forced;
   DBuf<int> cnt(1, s);
   cnt.zero();
   out.lrows.alloc(A.n > 0 ? A.n : 1, s);
@@ -487,6 +488,10 @@ static void spmv_dispatch(const DevMat<T>& A, const T* x, const T* b, T* y, cuda
     case 8:
       BN_LAUNCH_PDL((k_spmv_vec<T, 8, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
                 dw, partial, skip);
+      break;
+    case 16:
+      BN_LAUNCH_PDL((k_spmv_vec<T, 16, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b,
+                    y, dw, partial, skip);
       break;
     default:
       BN_LAUNCH_PDL((k_spmv_vec<T, 32, MODE, DOT>), grid, 256, 0, s, A.ia, A.ja, A.val, x, A.n, b, y,
@@ -643,23 +648,38 @@ static void gs_launch(const DevMat<T>& A, const int* rows, int r0, int nr, const
     return;
   }
   if (group == 0) group = 1;
+  const int lanes = group >= 32 ? 32 : group >= 16 ? 16 : group >= 8 ? 8 : group >= 4 ? 4
+                                                                                      : group >= 2 ? 2 : 1;
   const int nshort = nr - nlong;
   int nb = 0;
-  if (nshort > 0)
-    nb = group >= 32 ? grid_for((long long)nshort * 32, kLongThreads, 8)
-                     : (group >= 8 ? grid_for((long long)nshort * 8, kLongThreads, 8)
-                                   : grid_for(nshort, kLongThreads, 8));
+  if (nshort > 0) nb = grid_for((long long)nshort * lanes, kLongThreads, 8);
   const int grid = nb + nlong;
   if (grid == 0) return;
-  if (group >= 32)
-    BN_LAUNCH_PDL((k_gs_class<T, 32>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
-              nb, b, x, out);
-  else if (group >= 8)
-    BN_LAUNCH_PDL((k_gs_class<T, 8>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
-              nb, b, x, out);
-  else
-    BN_LAUNCH_PDL((k_gs_class<T, 1>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0, nshort,
-              nb, b, x, out);
+  switch (lanes) {
+    case 32:
+      BN_LAUNCH_PDL((k_gs_class<T, 32>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+      break;
+    case 16:
+      BN_LAUNCH_PDL((k_gs_class<T, 16>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+      break;
+    case 8:
+      BN_LAUNCH_PDL((k_gs_class<T, 8>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+      break;
+    case 4:
+      BN_LAUNCH_PDL((k_gs_class<T, 4>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+      break;
+    case 2:
+      BN_LAUNCH_PDL((k_gs_class<T, 2>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+      break;
+    default:
+      BN_LAUNCH_PDL((k_gs_class<T, 1>), grid, kLongThreads, 0, s, A.ia, A.ja, A.val, rows, r0,
+                    nshort, nb, b, x, out);
+  }
 }
 
 template <class T>

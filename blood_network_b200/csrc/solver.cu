@@ -423,10 +423,11 @@ void Solver::color_level(Level& L, int smoother) {
   }
   const double avg = n > 0 ? (double)L.A.nnz / n : 0.0;
   L.gs_group = avg <= 12.0 ? 1 : (avg <= 48.0 ? 8 : 32);
-  // BN_GS_LANES=g pins the Gauss-Seidel kernel (0 staged row tiles, 1/8/32
-  // lanes per row); the autotuner may still change it
+  // BN_GS_LANES=g pins the Gauss-Seidel kernel (0 staged row tiles, 1/2/4/8/
+  // 16/32 lanes per row); the autotuner may still change it
   static const int gs_forced = getenv("BN_GS_LANES") ? atoi(getenv("BN_GS_LANES")) : -1;
-  if (gs_forced == 0 || gs_forced == 1 || gs_forced == 8 || gs_forced == 32)
+  if (gs_forced == 0 || gs_forced == 1 || gs_forced == 2 || gs_forced == 4 || gs_forced == 8 ||
+      gs_forced == 16 || gs_forced == 32)
     L.gs_group = gs_forced;
 }
 
@@ -2066,7 +2067,7 @@ int Solver::autotune_t(int what, double* report, int nreport) {
         if (op.packed || op.M->n == 0) continue;
         int best = op.lay->group;
         double best_ms = 1e30;
-        for (int g : {0, 1, 2, 3, 4, 5, 8, 32}) {
+        for (int g : {0, 1, 2, 3, 4, 5, 8, 16, 32}) {
           op.lay->group = g;
           DevMat<T> M = mat<T>(*op.M, op.v32, op.lay);
           const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
@@ -2083,7 +2084,7 @@ int Solver::autotune_t(int what, double* report, int nreport) {
         !(use_packed && L.use_pkA)) {
       int best = L.gs_group;
       double best_ms = 1e30;
-      for (int g : {0, 1, 8, 32}) {  // 0: staged row tiles
+      for (int g : {0, 1, 2, 4, 8, 16, 32}) {  // 0: staged row tiles
         L.gs_group = g;
         const double ms = time_ms<T>(s, ev0, ev1, reps, [&]() {
           smooth<T>(l, v.p, u.p, true);

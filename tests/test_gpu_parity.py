@@ -320,9 +320,9 @@ def test_bench_kernel_timings(net20k):
 @pytest.mark.parametrize("precision", [amg.PREC_FP64, amg.PREC_MIXED])
 def test_autotuner_choices(net20k, precision):
     """amg_solver_autotune keeps, per level operator, the fastest candidate
-    (SpMV row tiles 0-3, staged tiles 5, lanes per row 4/8/32; GS lanes
-    1/8/32), for A, R, P and the split residual operator; the solve still converges
-    with the same work."""
+    (SpMV row tiles 0-3, staged tiles 5, lanes per row 4/8/16/32; GS staged
+    tiles 0 or lanes 1/2/4/8/16/32), for A, R, P and the split residual
+    operator; the solve still converges with the same work."""
     s = _solver(net20k.n, net20k.indptr, net20k.indices, net20k.data, precision=precision)
     x0, it0 = s.solve(net20k.rhs, tol=1e-8)
     rep = s.autotune(3)
@@ -330,9 +330,9 @@ def test_autotuner_choices(net20k, precision):
     for lvl, op, choice, ms in rep:
         assert 0 <= lvl < s.num_levels - 1 and ms > 0
         if op == 3:
-            assert choice in (0, 1, 8, 32)       # Gauss-Seidel: staged tiles, lanes per row
+            assert choice in (0, 1, 2, 4, 8, 16, 32)  # Gauss-Seidel: staged tiles, lanes per row
         else:
-            assert choice in (0, 1, 2, 3, 4, 5, 8, 32)  # SpMV forms (5: staged tiles)
+            assert choice in (0, 1, 2, 3, 4, 5, 8, 16, 32)  # SpMV forms (5: staged tiles)
     x1, it1 = s.solve(net20k.rhs, tol=1e-8)
     assert abs(it1 - it0) <= 1
     assert relres(net20k.indptr, net20k.indices, net20k.data, x1, net20k.rhs) <= 1e-8
@@ -487,3 +487,48 @@ def test_ic_slab_form_on_a_large_network():
     assert forms == [[2, 2], [4, 4], [5, 5]]
     for r in res[1:]:
         assert r.tobytes() == res[0].tobytes()
+
+
+def test_lanes_per_row_variants_converge():
+    """Every lanes-per-row variant of the coloured Gauss-Seidel (BN_GS_LANES
+    1/2/4/8/16/32) and of the group SpMV (BN_SPMV_GROUP 4/8/16/32) sums a
+    row's products over its lanes with a fixed shuffle tree, so a variant
+    changes only the rounding of the smoother and the coarse operators'
+    products: whole solves reach the tolerance with the iteration count
+    within one of the default's, in both precisions."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from blood_network_b200 import amg\n"
+        "from blood_network_b200.network import make_config\n"
+        "net = make_config('vascular_20k')\n"
+        "its = []\n"
+        "for prec in (amg.PREC_FP64, amg.PREC_MIXED):\n"
+        "    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=prec,\n"
+        "                      stop=amg.STOP_RELRES)\n"
+        "    x, it = s.solve(net.rhs, tol=1e-8)\n"
+        "    its.append(it)\n"
+        "    np.save(sys.argv[1] + '.%%d.npy' %% prec, x)\n"
+        "np.save(sys.argv[1], np.array(its))\n" % root)
+    net = make_config("vascular_20k")
+    runs = [{}] + [{"BN_GS_LANES": g} for g in ("1", "2", "4", "8", "16", "32")] + \
+        [{"BN_SPMV_GROUP": g} for g in ("4", "8", "16", "32")]
+    its = []
+    for k, extra in enumerate(runs):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"lanes_{k}_{os.getpid()}.npy")
+        env = dict(os.environ)
+        env.pop("BN_GS_LANES", None)
+        env.pop("BN_SPMV_GROUP", None)
+        env.update(extra)
+        subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600, env=env)
+        its.append(np.load(path))
+        os.remove(path)
+        for prec in (0, 1):
+            x = np.load(path + ".%d.npy" % prec)
+            os.remove(path + ".%d.npy" % prec)
+            assert relres(net.indptr, net.indices, net.data, x, net.rhs) <= 1e-8
+    for it in its[1:]:
+        assert np.all(np.abs(it - its[0]) <= 1)
