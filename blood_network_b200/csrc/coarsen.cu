@@ -323,6 +323,69 @@ __global__ void k_count_c(const int* __restrict__ cf, int n, int* counter) {
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(counter, local);
 }
 
+// The first n draws of rand() after srand(seed) (crand.h), on the device:
+// thread j produces draws [j C, (j+1) C) from its starting window, which it
+// forms from the first window and the jump matrices of j's set bits.
+constexpr int kCrandStep = 2048;  // draws per thread (a multiple of 32)
+
+__global__ void __launch_bounds__(128)
+k_crand_chunks(const uint32_t* __restrict__ pw, int nbits, const uint32_t* __restrict__ first,
+               long long n, int* __restrict__ out) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j * kCrandStep >= n) return;
+  uint32_t v[31];
+#pragma unroll
+  for (int i = 0; i < 31; i++) v[i] = first[i];
+  for (int b = 0; b < nbits; b++) {
+    if (!((j >> b) & 1)) continue;
+    const uint32_t* m = pw + (size_t)b * 961;
+    uint32_t t[31];
+#pragma unroll
+    for (int i = 0; i < 31; i++) {
+      uint32_t acc = 0;
+#pragma unroll
+      for (int k = 0; k < 31; k++) acc += m[i * 31 + k] * v[k];
+      t[i] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < 31; i++) v[i] = t[i];
+  }
+  // ring slot (q & 31) holds position q of the chunk (q = -31 .. -1 first)
+  uint32_t ring[32];
+  ring[0] = 0;
+#pragma unroll
+  for (int i = 1; i < 32; i++) ring[i] = v[i - 1];
+  const long long base = j * kCrandStep;
+  for (int q0 = 0; q0 < kCrandStep; q0 += 32) {
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      const uint32_t r = ring[(i + 1) & 31] + ring[(i + 29) & 31];  // r[q-31] + r[q-3]
+      ring[i] = r;
+      const long long k = base + q0 + i;
+      if (k < n) out[k] = (int)(r >> 1);
+    }
+  }
+}
+
+static void crand_device(unsigned seed, int* out, long long n, cudaStream_t s) {
+  if (n <= 0) return;
+  const long long nchunks = (n + kCrandStep - 1) / kCrandStep;
+  int nbits = 1;
+  while ((1LL << nbits) < nchunks) nbits++;
+  std::vector<CrandMat> pw(nbits);
+  crand_jump_matrices(kCrandStep, nbits, pw.data());
+  std::vector<uint32_t> h((size_t)nbits * 961 + 31);
+  for (int b = 0; b < nbits; b++)
+    for (int i = 0; i < 31; i++)
+      for (int k = 0; k < 31; k++) h[(size_t)b * 961 + i * 31 + k] = pw[b].a[i][k];
+  crand_first_window(seed, h.data() + (size_t)nbits * 961);
+  DBuf<uint32_t> d(h.size(), s);
+  d.upload(h.data(), h.size());
+  BN_LAUNCH(k_crand_chunks, (int)((nchunks + 127) / 128), 128, 0, s, d.p, nbits,
+            d.p + (size_t)nbits * 961, n, out);
+  BN_CUDA(cudaStreamSynchronize(s));  // h must outlive the copy
+}
+
 static void select_round(const CSR& S, const CSR& T, const double* w, int n, int* cf,
                          const int* longs, int nlong, int glong, int* ctr, cudaStream_t s) {
   BN_LAUNCH(k_select, grid_for(n, 256), 256, 0, s, S.ia.p, S.ja.p, T.ia.p, T.ja.p, w, n, cf, ctr);
@@ -411,21 +474,18 @@ int coarsen(const CSR& S, int method, int max_lam, int* cf, cudaStream_t s) {
     // RS measure: lambda_i = |S^T_i|; the classical RS routine leaves
     // lambda_0 at zero (rs_classical.c:118-123), reproduced here.
     if (method == COARSEN_RS) BN_CUDA(cudaMemsetAsync(lam.p, 0, sizeof(int), s));
-    std::vector<int> h;
     DBuf<int> rnd;
     if (method == COARSEN_HMIS) {
       // ties between equal measures: the reference HMIS's weights
       // lambda_i + rand()/RAND_MAX after srand(12345) (rs_classical.c:
       // 542-551), one draw per point in index order.  The sequence comes
-      // from a restatement of the C library's generator (crand.h), so the
+      // from a restatement of the C library's generator (crand.h, drawn on the
+      // device in chunks from jump-ahead windows), so the
       // caller's rand() state is left alone as the reference's first pass
       // leaves it.
-      h.resize(n);
-      crand_sequence(12345u, h.data(), n);
       rnd.alloc(n, s);
-      rnd.upload(h.data(), n);
+      crand_device(12345u, rnd.p, n, s);
       BN_LAUNCH(k_pmis_weights, g, 256, 0, s, lam.p, rnd.p, n, w.p, cf);
-      BN_CUDA(cudaStreamSynchronize(s));  // h must outlive the copy
     } else {
       BN_LAUNCH(k_rs_measure, g, 256, 0, s, lam.p, n, w.p);
     }
