@@ -476,10 +476,13 @@ __global__ void k_row_class_start(const int* __restrict__ cptr, int ncls, int n,
     cs[i] = cptr[lo];
   }
 }
+// Rows longer than kLongRow (the hub rows, listed in the layout's lrows) are
+// left to the block-per-row kernels below.
 __global__ void k_split_count(const int* __restrict__ ia, const int* __restrict__ ja,
                               const int* __restrict__ cs, int n, int* __restrict__ cl,
                               int* __restrict__ cu) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (ia[i + 1] - ia[i] > kLongRow) continue;
     int nlow = 0, nall = 0;
     for (int k = ia[i]; k < ia[i + 1]; k++) {
       const int j = ja[k];
@@ -496,6 +499,7 @@ __global__ void k_split_fill(const int* __restrict__ ia, const int* __restrict__
                              double* __restrict__ la, const int* __restrict__ uia,
                              int* __restrict__ uja, double* __restrict__ ua) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (ia[i + 1] - ia[i] > kLongRow) continue;
     int pl = lia[i], pu = uia[i];
     for (int k = ia[i]; k < ia[i + 1]; k++) {
       const int j = ja[k];
@@ -510,6 +514,74 @@ __global__ void k_split_fill(const int* __restrict__ ia, const int* __restrict__
   }
 }
 
+// A block per long row: counts, then the entries in chunks of blockDim.x,
+// each chunk's AL entries placed by a block-wide prefix of the split flags
+// (so both parts keep the row's order).
+__global__ void __launch_bounds__(256)
+k_split_count_long(const int* __restrict__ ia, const int* __restrict__ ja,
+                   const int* __restrict__ cs, const int* __restrict__ lrows,
+                   int* __restrict__ cl, int* __restrict__ cu) {
+  __shared__ int red[8];
+  const int i = lrows[blockIdx.x];
+  const int c = cs[i];
+  int nlow = 0;
+  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += blockDim.x) {
+    const int j = ja[k];
+    nlow += (j < c || j == i);
+  }
+  for (int off = 16; off > 0; off >>= 1) nlow += __shfl_xor_sync(0xffffffffu, nlow, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nlow;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    cl[i] = t;
+    cu[i] = (ia[i + 1] - ia[i]) - t;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_split_fill_long(const int* __restrict__ ia, const int* __restrict__ ja,
+                  const double* __restrict__ a, const int* __restrict__ cs,
+                  const int* __restrict__ lrows, const int* __restrict__ lia,
+                  int* __restrict__ lja, double* __restrict__ la, const int* __restrict__ uia,
+                  int* __restrict__ uja, double* __restrict__ ua) {
+  __shared__ int wsum[8];
+  const int i = lrows[blockIdx.x];
+  const int c = cs[i];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int pl = lia[i], pu = uia[i];
+  for (int k0 = ia[i]; k0 < ia[i + 1]; k0 += blockDim.x) {
+    const int k = k0 + threadIdx.x;
+    const bool in = k < ia[i + 1];
+    const int j = in ? ja[k] : 0;
+    const bool low = in && (j < c || j == i);
+    const unsigned bal = __ballot_sync(0xffffffffu, low);
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int q = 0; q < nw; q++) {
+      before += q < w ? wsum[q] : 0;
+      total += wsum[q];
+    }
+    const int rank = before + __popc(bal & ((1u << lane) - 1u));  // AL entries before k
+    if (in) {
+      if (low) {
+        lja[pl + rank] = j;
+        la[pl + rank] = a[k];
+      } else {
+        const int r = (k - k0) - rank;
+        uja[pu + r] = j;
+        ua[pu + r] = -a[k];
+      }
+    }
+    const int chunk = (ia[i + 1] - k0) < (int)blockDim.x ? ia[i + 1] - k0 : (int)blockDim.x;
+    pl += total;
+    pu += chunk - total;
+    __syncthreads();
+  }
+}
+
 // AL / AU of a coloured level (entries keep their order within each part)
 void Solver::build_split(Level& L) {
   const CSR& A = L.Ap;
@@ -521,6 +593,10 @@ void Solver::build_split(Level& L) {
   cu.zero();
   BN_LAUNCH(k_row_class_start, g, 256, 0, s, L.d_cptr.p, ncls, n, cs.p);
   BN_LAUNCH(k_split_count, g, 256, 0, s, A.ia.p, A.ja.p, cs.p, n, cl.p, cu.p);
+  const int nlong = L.layA.nlong;  // rows of Ap longer than kLongRow
+  if (nlong > 0)
+    BN_LAUNCH(k_split_count_long, nlong, 256, 0, s, A.ia.p, A.ja.p, cs.p, L.layA.lrows.p, cl.p,
+              cu.p);
   const int nl = scan_counts(cl.p, n, s);
   const int nu = scan_counts(cu.p, n, s);
   L.AL.n = L.AU.n = n;
@@ -535,6 +611,9 @@ void Solver::build_split(Level& L) {
   L.AU.val.alloc(nu > 0 ? nu : 1, s);
   BN_LAUNCH(k_split_fill, g, 256, 0, s, A.ia.p, A.ja.p, A.val.p, cs.p, n, L.AL.ia.p, L.AL.ja.p,
             L.AL.val.p, L.AU.ia.p, L.AU.ja.p, L.AU.val.p);
+  if (nlong > 0)
+    BN_LAUNCH(k_split_fill_long, nlong, 256, 0, s, A.ia.p, A.ja.p, A.val.p, cs.p,
+              L.layA.lrows.p, L.AL.ia.p, L.AL.ja.p, L.AL.val.p, L.AU.ia.p, L.AU.ja.p, L.AU.val.p);
   analyze_rows(L.AL, L.layAL, s);
   analyze_rows(L.AU, L.layAU, s);
   order_tiles(n, L.perm.p, L.layAL, s);
