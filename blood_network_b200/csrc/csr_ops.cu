@@ -445,9 +445,99 @@ void add_scaled(const CSR& A, const CSR& B, double scale, CSR& C, cudaStream_t s
   }
 }
 
+// (A + A^T) / 2 of a structurally symmetric A.  The reference's merge-add
+// (row i of A, then the entries of row i of A^T that A's row lacks, times
+// 0.5; agg_lib.h dcsr_mat_add, build_hierarchy.c:116-126) appends nothing
+// then, so the result keeps A's pattern and entry order with
+// c_ij = (a_ij + a_ji) * 0.5; a_ji is found by binary search in row i of A^T,
+// whose columns are increasing (the transpose keeps rows in order).  A
+// thread per row; rows longer than kSymLong go to a block each.  A missing
+// a_ji sets *asym and the general merge-add runs instead.
+constexpr int kSymLong = 256;
+
+__device__ __forceinline__ int sym_find(const int* __restrict__ tja, int lo, int hi, int key) {
+  int a = lo, b = hi;
+  while (a < b) {
+    const int mid = (a + b) >> 1;
+    if (tja[mid] < key) a = mid + 1;
+    else b = mid;
+  }
+  return (a < hi && tja[a] == key) ? a : -1;
+}
+
+__global__ void k_sym_rows(const int* __restrict__ ia, const int* __restrict__ ja,
+                           const double* __restrict__ a, const int* __restrict__ tia,
+                           const int* __restrict__ tja, const double* __restrict__ ta, int n,
+                           double* __restrict__ out, int* __restrict__ asym,
+                           int* __restrict__ longs, int* __restrict__ nlong) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int k0 = ia[i], k1 = ia[i + 1];
+    if (tia[i + 1] - tia[i] != k1 - k0) {
+      atomicOr(asym, 1);
+      continue;
+    }
+    if (k1 - k0 > kSymLong) {
+      longs[atomicAdd(nlong, 1)] = i;
+      continue;
+    }
+    for (int k = k0; k < k1; k++) {
+      const int p = sym_find(tja, tia[i], tia[i + 1], ja[k]);
+      if (p < 0) {
+        atomicOr(asym, 1);
+        break;
+      }
+      out[k] = xmul(xadd(a[k], ta[p]), 0.5);
+    }
+  }
+}
+
+__global__ void k_sym_long(const int* __restrict__ ia, const int* __restrict__ ja,
+                           const double* __restrict__ a, const int* __restrict__ tia,
+                           const int* __restrict__ tja, const double* __restrict__ ta,
+                           const int* __restrict__ longs, double* __restrict__ out,
+                           int* __restrict__ asym) {
+  const int i = longs[blockIdx.x];
+  for (int k = ia[i] + threadIdx.x; k < ia[i + 1]; k += blockDim.x) {
+    const int p = sym_find(tja, tia[i], tia[i + 1], ja[k]);
+    if (p < 0) {
+      atomicOr(asym, 1);
+      continue;
+    }
+    out[k] = xmul(xadd(a[k], ta[p]), 0.5);
+  }
+}
+
 void symmetrize(const CSR& A, CSR& out, cudaStream_t s) {
   CSR T;
   transpose(A, T, s, true);
+  const int n = A.n;
+  if (n > 0 && A.n == A.m && A.nnz > 0) {
+    DBuf<int> flags(2, s), longs(n, s);
+    flags.zero();
+    out.n = A.n;
+    out.m = A.m;
+    out.nnz = A.nnz;
+    out.ia.alloc((size_t)n + 1, s);
+    out.ja.alloc((size_t)A.nnz, s);
+    out.val.alloc((size_t)A.nnz, s);
+    BN_LAUNCH(k_sym_rows, grid_for(n, 256), 256, 0, s, A.ia.p, A.ja.p, A.val.p, T.ia.p, T.ja.p,
+              T.val.p, n, out.val.p, flags.p, longs.p, flags.p + 1);
+    int h[2];
+    flags.download(h, 2);
+    BN_CUDA(cudaStreamSynchronize(s));
+    if (!h[0] && h[1] > 0)
+      BN_LAUNCH(k_sym_long, h[1], 256, 0, s, A.ia.p, A.ja.p, A.val.p, T.ia.p, T.ja.p, T.val.p,
+                longs.p, out.val.p, flags.p);
+    if (!h[0] && h[1] > 0) h[0] = read_scalar(flags.p, s);
+    if (!h[0]) {
+      BN_CUDA(cudaMemcpyAsync(out.ia.p, A.ia.p, sizeof(int) * ((size_t)n + 1),
+                              cudaMemcpyDeviceToDevice, s));
+      BN_CUDA(cudaMemcpyAsync(out.ja.p, A.ja.p, sizeof(int) * (size_t)A.nnz,
+                              cudaMemcpyDeviceToDevice, s));
+      return;
+    }
+    out = CSR();
+  }
   add_scaled(A, T, 0.5, out, s);
 }
 
