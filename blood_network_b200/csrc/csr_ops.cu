@@ -450,10 +450,11 @@ void add_scaled(const CSR& A, const CSR& B, double scale, CSR& C, cudaStream_t s
 // 0.5; agg_lib.h dcsr_mat_add, build_hierarchy.c:116-126) appends nothing
 // then, so the result keeps A's pattern and entry order with
 // c_ij = (a_ij + a_ji) * 0.5; a_ji is found by binary search in row i of A^T,
-// whose columns are increasing (the transpose keeps rows in order).  A
-// thread per row; rows longer than kSymLong go to a block each.  A missing
-// a_ji sets *asym and the general merge-add runs instead.
-constexpr int kSymLong = 256;
+// whose columns are increasing (the transpose keeps rows in order).  A warp
+// per row, its lanes striding the row's entries; rows longer than kSymLong
+// go to a block each.  A missing a_ji sets *asym and the general merge-add
+// runs instead.
+constexpr int kSymLong = 1024;
 
 __device__ __forceinline__ int sym_find(const int* __restrict__ tja, int lo, int hi, int key) {
   int a = lo, b = hi;
@@ -470,21 +471,24 @@ __global__ void k_sym_rows(const int* __restrict__ ia, const int* __restrict__ j
                            const int* __restrict__ tja, const double* __restrict__ ta, int n,
                            double* __restrict__ out, int* __restrict__ asym,
                            int* __restrict__ longs, int* __restrict__ nlong) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     const int k0 = ia[i], k1 = ia[i + 1];
     if (tia[i + 1] - tia[i] != k1 - k0) {
-      atomicOr(asym, 1);
+      if (lane == 0) atomicOr(asym, 1);
       continue;
     }
     if (k1 - k0 > kSymLong) {
-      longs[atomicAdd(nlong, 1)] = i;
+      if (lane == 0) longs[atomicAdd(nlong, 1)] = i;
       continue;
     }
-    for (int k = k0; k < k1; k++) {
-      const int p = sym_find(tja, tia[i], tia[i + 1], ja[k]);
+    const int t0 = tia[i], t1 = tia[i + 1];
+    for (int k = k0 + lane; k < k1; k += 32) {
+      const int p = sym_find(tja, t0, t1, ja[k]);
       if (p < 0) {
         atomicOr(asym, 1);
-        break;
+        continue;
       }
       out[k] = xmul(xadd(a[k], ta[p]), 0.5);
     }
@@ -520,7 +524,7 @@ void symmetrize(const CSR& A, CSR& out, cudaStream_t s) {
     out.ia.alloc((size_t)n + 1, s);
     out.ja.alloc((size_t)A.nnz, s);
     out.val.alloc((size_t)A.nnz, s);
-    BN_LAUNCH(k_sym_rows, grid_for(n, 256), 256, 0, s, A.ia.p, A.ja.p, A.val.p, T.ia.p, T.ja.p,
+    BN_LAUNCH(k_sym_rows, grid_for((long long)n * 32, 256), 256, 0, s, A.ia.p, A.ja.p, A.val.p, T.ia.p, T.ja.p,
               T.val.p, n, out.val.p, flags.p, longs.p, flags.p + 1);
     int h[2];
     flags.download(h, 2);
