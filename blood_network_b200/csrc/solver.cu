@@ -371,7 +371,9 @@ void Solver::color_level(Level& L, int smoother) {
                 ctr.p, cap);
     }
     BN_LAUNCH(k_color_commit, g, 256, 0, s, n, newc.p, color.p);
-    done += read_scalar(ctr.p, s);
+    // capped levels run their rounds without asking how many rows are left
+    // (a round with nothing left to colour changes nothing)
+    if (cap >= kMaxColors) done += read_scalar(ctr.p, s);
     round++;
   }
   DBuf<int> key(n, s), ids(n, s), key_out(n, s);
