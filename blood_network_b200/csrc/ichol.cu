@@ -423,30 +423,84 @@ k_tri_flags(const int* __restrict__ ia, const int* __restrict__ ja, const T* __r
       T s = in[i];
       const T d = diag[t];
       if (clear) reinterpret_cast<U*>(clear)[i] = W::kPending;
-      for (int k = k0; k < k1; k += 4) {
-        const int m = k1 - k < 4 ? k1 - k : 4;
+      if (k1 - k0 <= 4) {
+        // at most one group (nearly every row): the row is computed and
+        // published inside its own polling loop, in the iteration its last
+        // dependency arrives, instead of after the warp has reconverged
+        // behind the chunk's slowest row
+        const int m = k1 - k0;
         int j[4];
         T v[4];
         U u[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          j[q] = q < m ? ja[k + q] : 0;
-          v[q] = q < m ? val[k + q] : T(0);
+          j[q] = q < m ? ja[k0 + q] : 0;
+          v[q] = q < m ? val[k0 + q] : T(0);
+          u[q] = U(0);
         }
+        unsigned long long t0 = 0;
+        for (int it = 0;; it++) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) u[q] = q < m ? ld_relaxed(o + j[q]) : U(0);
-        wait_group(o, j, u, m, W::kPending, W::kNaN, wc, i);
+          for (int q = 0; q < 4; q++)
+            if (q < m && (it == 0 || u[q] == W::kPending)) u[q] = ld_relaxed(o + j[q]);
+          bool pend = false;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          if (q < m) {
-            if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[q], word_value(u[q])));
-            else s = xsubf(s, xmulf(v[q], word_value(u[q])));
+          for (int q = 0; q < 4; q++) pend |= (q < m && u[q] == W::kPending);
+          bool give_up = false;
+          if (pend && it >= kSpinFast) {
+            bool ran_out = false;
+            if (wait_backoff(wc, it, t0, &ran_out)) {
+              int dep = -1;
+#pragma unroll
+              for (int q = 3; q >= 0; q--)
+                if (q < m && u[q] == W::kPending) dep = j[q];
+              if (ran_out) wait_give_up(wc, i, dep, global_ns() - t0);
+#pragma unroll
+              for (int q = 0; q < 4; q++)
+                if (q < m && u[q] == W::kPending) u[q] = W::kNaN;
+              give_up = true;
+            }
+          }
+          if (!pend || give_up) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              if (q < m) {
+                if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[q], word_value(u[q])));
+                else s = xsubf(s, xmulf(v[q], word_value(u[q])));
+              }
+            }
+            U r = value_word(s / d);
+            if (r == W::kPending) r = W::kNaN;
+            st_relaxed(o + i, r);
+            break;
           }
         }
+      } else {
+        for (int k = k0; k < k1; k += 4) {
+          const int m = k1 - k < 4 ? k1 - k : 4;
+          int j[4];
+          T v[4];
+          U u[4];
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            j[q] = q < m ? ja[k + q] : 0;
+            v[q] = q < m ? val[k + q] : T(0);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++) u[q] = q < m ? ld_relaxed(o + j[q]) : U(0);
+          wait_group(o, j, u, m, W::kPending, W::kNaN, wc, i);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            if (q < m) {
+              if constexpr (sizeof(T) == 8) s = xsub(s, xmul(v[q], word_value(u[q])));
+              else s = xsubf(s, xmulf(v[q], word_value(u[q])));
+            }
+          }
+        }
+        U r = value_word(s / d);
+        if (r == W::kPending) r = W::kNaN;
+        st_relaxed(o + i, r);
       }
-      U r = value_word(s / d);
-      if (r == W::kPending) r = W::kNaN;
-      st_relaxed(o + i, r);
     }
     __syncwarp();
   }
