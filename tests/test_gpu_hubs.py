@@ -277,6 +277,42 @@ def test_symmetrize_huge_rows():
 
 
 @pytest.mark.gpu
+def test_symmetrize_symmetric_pattern_with_a_hub_row():
+    """A structurally symmetric matrix with unequal a_ij and a_ji keeps its
+    pattern and entry order, each value (a_ij + a_ji) * 0.5 (binary search in
+    the transpose's row; a block for the 3,000-entry hub row): equal to the
+    reference's merge-add bit for bit."""
+    rng = np.random.default_rng(11)
+    n = 12000
+    rows = [dict() for _ in range(n)]
+    for i in range(n):
+        rows[i][i] = 40.0 + rng.uniform(0.0, 1.0)
+    def link(i, j):
+        rows[i][j] = -rng.uniform(0.5, 1.5)
+        rows[j][i] = -rng.uniform(0.5, 1.5)  # same pattern, another value
+    for i in range(n - 1):
+        link(i, i + 1)
+    for j in rng.choice(np.arange(2, n), 3000, replace=False):
+        link(0, int(j))
+    rows[0][0] = 4000.0  # diagonally dominant hub row
+    ia, ja, val = [0], [], []
+    for i in range(n):
+        cols = list(rows[i].keys())
+        rng.shuffle(cols)  # rows in no particular column order
+        ja += cols
+        val += [rows[i][c] for c in cols]
+        ia.append(len(ja))
+    ia, ja, val = np.array(ia, np.int32), np.array(ja, np.int32), np.array(val)
+    want = reference_symmetrize(n, ia, ja, val)
+    assert np.array_equal(want[1], ja)  # the merge-add appends nothing
+    s = amg.AMGSolver(n, ia, ja, val, threshold=0.25)
+    got = s.level(0)["A"]
+    for a, b in zip(got, want):
+        assert np.asarray(a).tobytes() == np.asarray(b, dtype=np.asarray(a).dtype).tobytes()
+    s.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("long_len", [1100, 2500])
 def test_spmv_dropins_with_a_long_row_among_short_rows(oracle, long_len):
     """The reference's abyvg / abyvam / abyvcs (sparse_ops.c:19-56) with a row
