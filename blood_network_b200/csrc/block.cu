@@ -402,6 +402,99 @@ k_tri_tiles_m(const int* __restrict__ ia, const int* __restrict__ ja, const T* _
   }
 }
 
+// Sync-free form of a many-column sweep: the rows in level order, a warp
+// per row taken round-robin by the warps of a co-resident grid, lane c (and
+// c + 32) holding column c.  Every value of the output block doubles as its
+// ready flag; a lane polls its own column of up to four dependencies at a
+// time and publishes its column as soon as those are in (the columns are
+// independent, so a lane never waits for the others).  A warp only waits on
+// rows of lower levels (earlier positions), and the earliest unfinished row
+// has all its dependencies published, so the sweep always advances; every
+// wait is bounded (flags.cuh).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_tri_flags_m(const int* __restrict__ ia, const int* __restrict__ ja, const T* __restrict__ val,
+              const T* __restrict__ diag, const int* __restrict__ rows, int n,
+              const T* __restrict__ in, T* out, int K, WaitCtl wc) {
+  using W = WordOf<T>;
+  using U = typename W::U;
+  U* o = reinterpret_cast<U*>(out);
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int t = warp; t < n; t += nw) {
+    const int i = rows[t];
+    const int k0 = ia[t], k1 = ia[t + 1];
+    const T d = diag[t];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int c = lane + 32 * h;
+      if (c >= K) continue;
+      T sum = in[(size_t)i * K + c];
+      for (int k = k0; k < k1; k += 4) {
+        const int m = k1 - k < 4 ? k1 - k : 4;
+        int jj[4];
+        T v[4];
+        U u[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          jj[q] = q < m ? ja[k + q] * K + c : 0;
+          v[q] = q < m ? val[k + q] : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) u[q] = q < m ? ld_relaxed(o + jj[q]) : U(0);
+        wait_group(o, jj, u, m, W::kPending, W::kNaN, wc, i);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (q < m) {
+            if constexpr (sizeof(T) == 8) sum = xsub(sum, xmul(v[q], word_value(u[q])));
+            else sum = xsubf(sum, xmulf(v[q], word_value(u[q])));
+          }
+        }
+      }
+      U r = value_word(sum / d);
+      if (r == W::kPending) r = W::kNaN;
+      st_relaxed(o + (size_t)i * K + c, r);
+    }
+  }
+}
+
+template <class T>
+static void sweep_flags_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
+  const int* ia = fwd ? ic.fia.p : ic.bia.p;
+  const int* ja = fwd ? ic.vfja.p : ic.vbja.p;
+  const int* rows = fwd ? ic.vorder.p : ic.vborder.p;
+  const T* val;
+  const T* diag;
+  if constexpr (sizeof(T) == 8) {
+    val = fwd ? ic.fval.p : ic.bval.p;
+    diag = fwd ? ic.fdiag.p : ic.bdiag.p;
+  } else {
+    val = fwd ? ic.fval32.p : ic.bval32.p;
+    diag = fwd ? ic.fdiag32.p : ic.bdiag32.p;
+  }
+  BN_CUDA(cudaMemsetAsync(x, 0xFF, sizeof(T) * (size_t)ic.n * K, s));
+  int dev = 0, per_sm = 0, sms = 0;
+  BN_CUDA(cudaGetDevice(&dev));
+  BN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tri_flags_m<T>, 256, 0));
+  BN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm > 4) per_sm = 4;
+  const int grid = sms * per_sm;
+  BN_REQUIRE(grid > 0, BN_ERR_CUDA, "block IC(0): sweep grid does not fit");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(256);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;  // co-residency: waits always end
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  g_launch_count++;
+  BN_CUDA(cudaLaunchKernelEx(&cfg, k_tri_flags_m<T>, ia, ja, val, diag, rows, ic.n, in, x, K,
+                             ic.wait.ctl(fwd ? WT_IC_FWD : WT_IC_BWD)));
+}
+
 template <class T>
 static void sweep_tiles_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
   const IChol::Tiles& tl = fwd ? ic.tf : ic.tb;
@@ -443,12 +536,19 @@ static void sweep_tiles_m(const IChol& ic, bool fwd, const T* in, T* x, int K, c
 
 template <class T>
 void sweep_m(const IChol& ic, bool fwd, const T* in, T* x, int K, cudaStream_t s) {
-  // level launches by default; BN_BLOCK_IC_TILES=1 selects the tiled form
-  // (64 columns on the 5M network, same run: 13.4 ms per right-hand side for
-  // the whole block solve with it, 11.2 ms with level launches)
+  // the sync-free form by default (64 columns on the 5M network, mixed, true
+  // residual 1e-8, same run: 23.5 ms per right-hand side for the whole block
+  // solve, 24.7 ms with level launches, bit-identical); BN_BLOCK_IC_TILES=1
+  // selects the tiled form (13.4 against 11.2 ms for level launches in an
+  // earlier run), BN_BLOCK_IC_LEVELS=1 the level launches
   static const bool tiles = getenv("BN_BLOCK_IC_TILES") && atoi(getenv("BN_BLOCK_IC_TILES"));
   if (tiles && ic.tf.ntiles > 0 && (size_t)ic.n * K < (1ull << 31)) {
     sweep_tiles_m<T>(ic, fwd, in, x, K, s);
+    return;
+  }
+  static const bool levels = getenv("BN_BLOCK_IC_LEVELS") && atoi(getenv("BN_BLOCK_IC_LEVELS"));
+  if (!levels && (size_t)ic.n * K < (1ull << 31)) {
+    sweep_flags_m<T>(ic, fwd, in, x, K, s);
     return;
   }
   const int* ia = fwd ? ic.fia.p : ic.bia.p;

@@ -188,3 +188,42 @@ def test_block_pcg_hub_rows_and_errors():
         S.solve_block(np.zeros((n, 65)))
     X, its, rel, rc = S.solve_block(B, tol=1e-14, maxiter=2)
     assert rc == -4 and np.all(its == -2)
+
+
+@pytest.mark.gpu
+def test_block_ic_sweep_forms_agree():
+    """The block PCG's many-column IC(0) sweeps, sync-free (default), by level
+    launches (BN_BLOCK_IC_LEVELS=1) or tiled (BN_BLOCK_IC_TILES=1), compute
+    every column of every row in the same operation order: the block solves
+    agree bit for bit, in both precisions."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from blood_network_b200 import amg\n"
+        "from blood_network_b200.network import make_config\n"
+        "net = make_config('vascular_20k')\n"
+        "rng = np.random.default_rng(3)\n"
+        "B = np.asfortranarray(net.rhs[:, None] * rng.uniform(0.5, 1.5, (1, 40)))\n"
+        "out = []\n"
+        "for prec in (amg.PREC_FP64, amg.PREC_MIXED):\n"
+        "    s = amg.AMGSolver(net.n, net.indptr, net.indices, net.data, precision=prec)\n"
+        "    X, its, rel, rc = s.solve_block(B, tol=1e-8)\n"
+        "    assert rc == 0 and rel.max() <= 1e-8\n"
+        "    out.append(X)\n"
+        "    s.close()\n"
+        "np.save(sys.argv[1], np.stack(out))\n" % root)
+    res = []
+    for k, extra in enumerate([{}, {"BN_BLOCK_IC_LEVELS": "1"}, {"BN_BLOCK_IC_TILES": "1"}]):
+        path = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"blkic_{k}_{os.getpid()}.npy")
+        env = dict(os.environ)
+        env.pop("BN_BLOCK_IC_LEVELS", None)
+        env.pop("BN_BLOCK_IC_TILES", None)
+        env.update(extra)
+        subprocess.run([sys.executable, "-c", code, path], check=True, timeout=600, env=env)
+        res.append(np.load(path))
+        os.remove(path)
+    for r in res[1:]:
+        assert r.tobytes() == res[0].tobytes()
